@@ -1,0 +1,126 @@
+// Device arithmetic and data-movement helpers for sm_100a.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace btk {
+
+// ---------------------------------------------------------------------------
+// FP64 reciprocal square root for the pairwise kernels.
+//
+// Seed: the FP32 approximation rsqrt.approx.f32 (one MUFU op) of the FP32
+// number that shares x's exponent and top 20 mantissa bits. The FP32 bit
+// pattern is built from x's high word by integer re-biasing of the exponent
+// (11-bit bias 1023 -> 8-bit bias 127: subtract 896 << 23 after a 3-bit
+// shift), and the FP32 result is widened the same way in reverse. No
+// floating-point conversion instruction is issued.
+//
+// Refinement: with e = 1 - x*y^2, the third-order Householder step for
+// f(y) = y^-2 - x,  y' = y * (1 + e/2 + 3e^2/8), cubes the relative error
+// (|e| <~ 1e-6 from the seed and the truncated mantissa, so |e'| <~ 1e-18,
+// below FP64 rounding). 5 FP64 operations.
+//
+// Domain: x in the FP32 normal range [2^-126, 2^127]. The kernels guarantee it
+// with eps^2 >= 2^-126; callers with smaller eps use rsqrt_fp64_guarded.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double rsqrt_fp64(double x) {
+  const int hi = __double2hiint(x);
+  const float xf = __int_as_float((hi << 3) + 0x40000000);
+  float yf;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
+  const int yb = __float_as_int(yf);
+  double y = __hiloint2double((yb >> 3) + 0x38000000, yb << 29);
+  const double e = fma(-x, y * y, 1.0);
+  const double p = fma(0.375, e, 0.5);
+  return fma(y * e, p, y);
+}
+
+// Same, extended to x = 0 (-> +inf, matching 1/sqrt(0)) and to x below the
+// FP32 normal range (rare: only with eps^2 < 2^-126 and near-coincident points).
+__device__ __forceinline__ double rsqrt_fp64_guarded(double x) {
+  if (x < 1.1754943508222875e-38) return x == 0.0 ? __longlong_as_double(0x7ff0000000000000LL) : 1.0 / sqrt(x);
+  return rsqrt_fp64(x);
+}
+
+// FP64 reciprocal of a positive x in the FP32 normal range: FP32 MUFU seed
+// (same re-biasing as above) and one cubically convergent Newton-type step
+// y' = y + y*(e + e^2), e = 1 - x*y. 4 FP64 operations.
+__device__ __forceinline__ double rcp_fp64_pos(double x) {
+  const int hi = __double2hiint(x);
+  const float xf = __int_as_float((hi << 3) + 0x40000000);
+  float yf;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
+  const int yb = __float_as_int(yf);
+  const double y = __hiloint2double((yb >> 3) + 0x38000000, yb << 29);
+  const double e = fma(-x, y, 1.0);
+  return fma(y, fma(e, e, e), y);
+}
+
+__device__ __forceinline__ double rcp_fp64_pos_guarded(double x) {
+  if (x < 1.1754943508222875e-38) return x == 0.0 ? __longlong_as_double(0x7ff0000000000000LL) : 1.0 / x;
+  return rcp_fp64_pos(x);
+}
+
+// FP32 hardware approximations used by the mixed-precision kernels.
+__device__ __forceinline__ float rsqrt_fp32(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_fp32(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// ---------------------------------------------------------------------------
+// mbarrier + TMA bulk copies (cp.async.bulk, no tensor map, no multicast).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// Makes barrier initialisation visible to the async (TMA) proxy.
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: gives up after `limit` polls (each poll may itself suspend
+// for a hardware-chosen interval) and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Global -> shared bulk copy completing on `bar`. dst, src 16-byte aligned,
+// bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+}  // namespace btk

@@ -1,0 +1,104 @@
+// Kernel declarations and the device-side data layout shared by the
+// translation units.
+//
+// Device layout of one tree side (targets or sources):
+//   sorted points      : double4 {x, y, z, w}, leaves contiguous in panel order,
+//                        points of a leaf in ascending original index
+//                        (the order of panel_points_inside rows);
+//   perm[k]            : original index of sorted point k;
+//   leaf_begin[panel]  : first sorted point of a leaf (-1 for non-leaves);
+//   nodes_shift        : [panel][3][kMaxNodes] Chebyshev points
+//                        cos(pi/n*i)*r + c (src/bli_impl.hpp:66-77) — proxy
+//                        point coordinates;
+//   nodes_interp       : [panel][3][kMaxNodes] cos(pi*i/n)*r + c — the node set
+//                        interp_vals_bli evaluates with (src/bli_impl.hpp:25);
+//   xfer               : [panel][3][kMaxNodes][kMaxNodes]
+//                        xfer[c][d][i][a] = L^{parent(c)}_a(node_shift^c_{d,i}),
+//                        the 1-D factors of child->parent anterpolation and
+//                        parent->child interpolation.
+// Proxy weights: [panel][ipc] row-major, proxy index ((a*m)+b)*m+c with x
+// slowest (src/upward_pass_impl.hpp:161-168).
+#pragma once
+
+#include "btk_internal.h"
+
+namespace btk {
+
+constexpr int kNodeStride = kMaxNodes;                     // per-axis stride
+constexpr int kPanelNodes = 3 * kNodeStride;               // doubles per panel
+constexpr int kPanelXfer = 3 * kMaxNodes * kMaxNodes;      // doubles per panel
+
+struct DevPanel {  // compact device copy of what kernels need per panel
+  double lo[3], hi[3];
+  int parent, is_leaf, point_count, level;
+};
+
+// ---- interaction work lists -----------------------------------------------
+struct WorkItem {
+  int t_begin;         // first target in the T4 array
+  int t_count;         // targets in this tile
+  int e_begin, e_end;  // entry range
+  int s_total;         // sources over the entries
+  int flags;           // kItemProxyTargets | kItemAtomic
+  int pad0, pad1;
+};
+constexpr int kItemProxyTargets = 1;  // outputs go to proxy target weights
+constexpr int kItemAtomic = 2;        // another item shares these targets
+
+struct Entry {
+  int s_begin;  // first source in the S4 array
+  int s_count;
+};
+
+struct Ptr4 {
+  double* p[4];
+};
+
+struct InteractParams {
+  const WorkItem* items;
+  int n_items;
+  const Entry* entries;
+  const double4* S4;
+  const double4* T4;
+  const int* T_out;
+  double* out[4];  // point-target outputs, one per component
+  double* ptw[4];  // proxy-target outputs, one per component
+  double eps2;
+  double scale[4];
+  int* ticket;
+  int* status;
+};
+
+constexpr int kInteractThreads = 128;
+constexpr int kTargetsPerThread = 2;
+constexpr int kTile = kInteractThreads * kTargetsPerThread;  // targets per work item
+
+// ---- launchers (return cudaGetLastError of the launch) -----------------------
+cudaError_t launch_panel_geometry(int dim, int degree, int P, const DevPanel* panels, const double* ucos_shift,
+                                  const double* ucos_interp, double* nodes_shift, double* nodes_interp, double* xfer,
+                                  cudaStream_t s);
+cudaError_t launch_perm_from_inside(int n_leaves, const int* leaves, const int* leaf_begin, const int* point_count,
+                                    const int* inside, int thresh, int* perm, cudaStream_t s);
+cudaError_t launch_gather(int n, const int* perm, const double* x, const double* y, const double* z,
+                          const double* w, double4* out, cudaStream_t s);
+cudaError_t launch_leaf_moments(int dim, int degree, int n_leaves, const int* leaves, const int* leaf_begin,
+                                const int* point_count, const double4* pts, const double* nodes_interp, double* psw,
+                                cudaStream_t s);
+cudaError_t launch_c2p(int dim, int degree, int n_parents, const int* parents, const int* child,
+                       const double* xfer, double* psw, cudaStream_t s);
+cudaError_t launch_src_proxies(int dim, int degree, int n_clusters, const int* cluster_panels,
+                               const double* nodes_shift, const double* psw, double4* out, cudaStream_t s);
+cudaError_t launch_tgt_proxies(int dim, int degree, int n_clusters, const int* cluster_panels,
+                               const double* nodes_shift, double4* out, int* out_index, cudaStream_t s);
+cudaError_t launch_p2c(int dim, int degree, int ncomp, int n_children, const int* children, const int* parent_of,
+                       const double* xfer, Ptr4 ptw, int ptw_stride, cudaStream_t s);
+cudaError_t launch_l2p(int dim, int degree, int ncomp, int n_leaves, const int* leaves, const int* leaf_begin,
+                       const int* point_count, const double4* pts, const int* perm, const double* nodes_interp,
+                       Ptr4 ptw, Ptr4 out, cudaStream_t s);
+cudaError_t launch_interact(int dim, int kind, int precision, bool guard, const InteractParams& p, int grid,
+                            cudaStream_t s);
+int interact_blocks_per_sm(int dim, int kind, int precision, bool guard);
+cudaError_t launch_direct(int dim, int kind, double eps, int nt, const double* xt, const double* yt,
+                          const double* zt, int ns, const double4* src, double* out, cudaStream_t s);
+
+}  // namespace btk

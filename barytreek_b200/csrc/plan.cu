@@ -1,0 +1,934 @@
+// Host orchestration: tree sides on the device, interaction work lists, the
+// plan API and the reference-named drop-in entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace btk {
+
+namespace {
+
+// ---- device memory -----------------------------------------------------------
+// Allocations of one plan or one drop-in call; freed together (stream-ordered).
+struct Arena {
+  cudaStream_t stream = nullptr;
+  std::vector<void*> ptrs;
+  size_t bytes = 0;
+  explicit Arena(cudaStream_t s) : stream(s) {}
+  ~Arena() {
+    for (void* p : ptrs) cudaFreeAsync(p, stream);
+  }
+  template <class T>
+  btk_status alloc(T** out, size_t n) {
+    *out = nullptr;
+    if (n == 0) return BTK_OK;
+    void* p = nullptr;
+    BTK_CUDA(cudaMallocAsync(&p, n * sizeof(T), stream));
+    ptrs.push_back(p);
+    bytes += n * sizeof(T);
+    *out = static_cast<T*>(p);
+    return BTK_OK;
+  }
+  template <class T>
+  btk_status upload(T** out, const std::vector<T>& v) {
+    BTK_TRY(alloc(out, v.size()));
+    if (!v.empty()) BTK_CUDA(cudaMemcpyAsync(*out, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    return BTK_OK;
+  }
+};
+
+int ipow(int b, int e) {
+  int r = 1;
+  while (e-- > 0) r *= b;
+  return r;
+}
+
+int ncomp_of(int dim, int kind) { return kind == BTK_KIND_POT ? 1 : (kind == BTK_KIND_VEL ? 3 : 1 + dim); }
+
+int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
+
+// ---- one side of the tree on the device ---------------------------------------
+struct Side {
+  HostTree h;
+  int n_points = 0;
+  int degree = 0, m = 0, ipc = 0;
+  std::vector<int> leaf_begin;    // per panel (-1 for non-leaf)
+  std::vector<int> leaves;        // non-empty leaves, panel order
+  std::vector<int> clusters;      // non-leaf panels, panel order (proxy slots)
+  std::vector<int> cluster_slot;  // per panel (-1 for leaves)
+  std::vector<std::vector<int>> nonleaf_by_level, panels_by_level;
+  // device
+  DevPanel* d_panels = nullptr;
+  int *d_leaf_begin = nullptr, *d_point_count = nullptr, *d_leaves = nullptr, *d_clusters = nullptr;
+  int *d_child = nullptr, *d_parent = nullptr, *d_perm = nullptr;
+  double *d_nodes_shift = nullptr, *d_nodes_interp = nullptr, *d_xfer = nullptr;
+  std::vector<int*> d_nonleaf_by_level, d_panels_by_level;
+};
+
+// Unit Chebyshev points in the reference's two evaluation orders, on the host
+// with std::cos as the reference does: cos(pi/n*i) for bli_points_shift
+// (src/bli_impl.hpp:74) and cos(pi*i/n) for interp_vals_bli (:25).
+void unit_cosines(int n, std::vector<double>& shift, std::vector<double>& interp) {
+  const double pi = 3.141592653589793238462643383279502884;
+  shift.resize(n + 1);
+  interp.resize(n + 1);
+  for (int i = 0; i <= n; ++i) {
+    shift[i] = std::cos(pi / n * i);
+    interp[i] = std::cos(pi * i / n);
+  }
+}
+
+btk_status side_layout(Side& S, int n_points, int degree) {
+  const HostTree& h = S.h;
+  S.n_points = n_points;
+  S.degree = degree;
+  S.m = degree + 1;
+  S.ipc = ipow(S.m, h.dim);
+  S.leaf_begin.assign(h.panel_count, -1);
+  S.cluster_slot.assign(h.panel_count, -1);
+  S.leaves.clear();
+  S.clusters.clear();
+  long long acc = 0;
+  for (int i = 0; i < h.panel_count; ++i) {
+    if (h.is_leaf[i]) {
+      S.leaf_begin[i] = (int)acc;
+      acc += h.point_count[i];
+      if (h.point_count[i] > 0) S.leaves.push_back(i);
+    } else {
+      S.cluster_slot[i] = (int)S.clusters.size();
+      S.clusters.push_back(i);
+    }
+  }
+  BTK_CHECK(acc == n_points, BTK_ERR_INVALID_ARGUMENT,
+            "tree: leaf point counts do not add up to the number of points");
+  S.nonleaf_by_level.assign(h.levels, {});
+  S.panels_by_level.assign(h.levels, {});
+  for (int l = 0; l < h.levels; ++l)
+    for (int i = h.level_start[l]; i < h.level_start[l + 1]; ++i) {
+      BTK_CHECK(i >= 0 && i < h.panel_count, BTK_ERR_INVALID_ARGUMENT, "tree: level_start out of range");
+      S.panels_by_level[l].push_back(i);
+      if (!h.is_leaf[i]) S.nonleaf_by_level[l].push_back(i);
+    }
+  // Structural checks the kernels rely on.
+  const int nc = 1 << h.dim;
+  for (int i = 0; i < h.panel_count; ++i) {
+    if (!h.is_leaf[i]) {
+      for (int c = 0; c < nc; ++c) {
+        int ch = h.child[(size_t)i * nc + c];
+        BTK_CHECK(ch > i && ch < h.panel_count && h.parent[ch] == i, BTK_ERR_INVALID_ARGUMENT,
+                  "tree: inconsistent child/parent links");
+      }
+    }
+    if (i > 0) BTK_CHECK(h.parent[i] >= 0 && h.parent[i] < i, BTK_ERR_INVALID_ARGUMENT, "tree: bad parent link");
+  }
+  return BTK_OK;
+}
+
+btk_status side_upload(Side& S, Arena& A, const int* host_inside, const int* dev_inside, int thresh) {
+  const HostTree& h = S.h;
+  cudaStream_t st = A.stream;
+  std::vector<DevPanel> dp(h.panel_count);
+  for (int i = 0; i < h.panel_count; ++i) {
+    for (int d = 0; d < 3; ++d) {
+      dp[i].lo[d] = h.geom[i].lo[d];
+      dp[i].hi[d] = h.geom[i].hi[d];
+    }
+    dp[i].parent = h.parent[i];
+    dp[i].is_leaf = h.is_leaf[i];
+    dp[i].point_count = h.point_count[i];
+    dp[i].level = h.level[i];
+  }
+  BTK_TRY(A.upload(&S.d_panels, dp));
+  BTK_TRY(A.upload(&S.d_leaf_begin, S.leaf_begin));
+  BTK_TRY(A.upload(&S.d_point_count, h.point_count));
+  BTK_TRY(A.upload(&S.d_leaves, S.leaves));
+  BTK_TRY(A.upload(&S.d_clusters, S.clusters));
+  BTK_TRY(A.upload(&S.d_child, h.child));
+  BTK_TRY(A.upload(&S.d_parent, h.parent));
+  S.d_nonleaf_by_level.assign(h.levels, nullptr);
+  S.d_panels_by_level.assign(h.levels, nullptr);
+  for (int l = 0; l < h.levels; ++l) {
+    BTK_TRY(A.upload(&S.d_nonleaf_by_level[l], S.nonleaf_by_level[l]));
+    BTK_TRY(A.upload(&S.d_panels_by_level[l], S.panels_by_level[l]));
+  }
+  // Geometry: nodes and transfer factors.
+  std::vector<double> us, ui;
+  unit_cosines(S.degree, us, ui);
+  double *d_us = nullptr, *d_ui = nullptr;
+  BTK_TRY(A.upload(&d_us, us));
+  BTK_TRY(A.upload(&d_ui, ui));
+  BTK_TRY(A.alloc(&S.d_nodes_shift, (size_t)h.panel_count * kPanelNodes));
+  BTK_TRY(A.alloc(&S.d_nodes_interp, (size_t)h.panel_count * kPanelNodes));
+  BTK_TRY(A.alloc(&S.d_xfer, (size_t)h.panel_count * kPanelXfer));
+  BTK_CUDA(launch_panel_geometry(h.dim, S.degree, h.panel_count, S.d_panels, d_us, d_ui, S.d_nodes_shift,
+                                 S.d_nodes_interp, S.d_xfer, st));
+  // Leaf order permutation.
+  BTK_TRY(A.alloc(&S.d_perm, (size_t)std::max(S.n_points, 1)));
+  if (host_inside) {
+    std::vector<int> perm(S.n_points);
+    for (int L : S.leaves)
+      for (int j = 0; j < h.point_count[L]; ++j) {
+        int v = host_inside[(size_t)L * thresh + j];
+        BTK_CHECK(v >= 0 && v < S.n_points, BTK_ERR_INVALID_ARGUMENT, "panel_points_inside: index out of range");
+        perm[S.leaf_begin[L] + j] = v;
+      }
+    if (S.n_points) BTK_CUDA(cudaMemcpyAsync(S.d_perm, perm.data(), sizeof(int) * S.n_points, cudaMemcpyHostToDevice, st));
+  } else if (dev_inside) {
+    BTK_CUDA(launch_perm_from_inside((int)S.leaves.size(), S.d_leaves, S.d_leaf_begin, S.d_point_count, dev_inside,
+                                     thresh, S.d_perm, st));
+  }
+  return BTK_OK;
+}
+
+// Builds the leaf permutation from point_leaf_panel (stable counting sort:
+// ascending original index inside each leaf, the order of panel_points_inside).
+btk_status side_perm_from_leaf_of(Side& S, Arena& A, const std::vector<int>& leaf_of) {
+  std::vector<int> cursor(S.leaf_begin);
+  std::vector<int> perm(S.n_points);
+  for (int i = 0; i < S.n_points; ++i) {
+    int L = leaf_of[i];
+    BTK_CHECK(L >= 0 && L < S.h.panel_count && S.h.is_leaf[L], BTK_ERR_INVALID_ARGUMENT,
+              "point_leaf_panel: not a leaf panel");
+    int pos = cursor[L]++;
+    BTK_CHECK(pos < S.leaf_begin[L] + S.h.point_count[L], BTK_ERR_INVALID_ARGUMENT,
+              "point_leaf_panel: more points than the leaf's point_count");
+    perm[pos] = i;
+  }
+  if (S.n_points)
+    BTK_CUDA(cudaMemcpyAsync(S.d_perm, perm.data(), sizeof(int) * S.n_points, cudaMemcpyHostToDevice, A.stream));
+  return BTK_OK;
+}
+
+// ---- interaction work lists -------------------------------------------------
+struct WorkLists {
+  std::vector<WorkItem> items;
+  std::vector<Entry> entries;
+  int64_t evals[4] = {0, 0, 0, 0};
+};
+
+btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lists[4], const int counts[4],
+                      int grid_slots, WorkLists& W) {
+  const int ipc = S.ipc;
+  const int nt = T.n_points, ns = S.n_points;
+  const int Pt = T.h.panel_count, Ps = S.h.panel_count;
+  // Stable grouping of pairs by target panel: point targets take PP then PC
+  // pairs, proxy targets CP then CC, each in list order.
+  std::vector<int> head(Pt + 1, 0);
+  for (int t = 0; t < 4; ++t)
+    for (int i = 0; i < counts[t]; ++i) {
+      const btk_interact_pair& pr = lists[t][i];
+      BTK_CHECK(pr.target_panel >= 0 && pr.target_panel < Pt && pr.source_panel >= 0 && pr.source_panel < Ps,
+                BTK_ERR_INVALID_ARGUMENT, "interaction list: panel index out of range");
+      const bool tgt_cluster = t >= 2, src_cluster = (t & 1) != 0;
+      BTK_CHECK(tgt_cluster == !T.h.is_leaf[pr.target_panel] && src_cluster == !S.h.is_leaf[pr.source_panel],
+                BTK_ERR_INVALID_ARGUMENT,
+                "interaction list: pair type does not match the panels (PP/PC targets and PP/CP sources must be "
+                "leaves, the others non-leaf)");
+      head[pr.target_panel + 1]++;
+    }
+  for (int i = 0; i < Pt; ++i) head[i + 1] += head[i];
+  std::vector<Entry> grouped(head[Pt]);
+  std::vector<int> cur(head.begin(), head.end() - 1);
+  for (int t = 0; t < 4; ++t)
+    for (int i = 0; i < counts[t]; ++i) {
+      const btk_interact_pair& pr = lists[t][i];
+      const int sp = pr.source_panel, tp = pr.target_panel;
+      Entry e;
+      if (t & 1) {  // cluster source: its proxies
+        e.s_begin = ns + S.cluster_slot[sp] * ipc;
+        e.s_count = ipc;
+      } else {
+        e.s_begin = S.leaf_begin[sp];
+        e.s_count = S.h.point_count[sp];
+      }
+      const int64_t nt_pts = (t >= 2) ? ipc : T.h.point_count[tp];
+      W.evals[t] += nt_pts * (int64_t)e.s_count;
+      grouped[cur[tp]++] = e;
+    }
+  // Tiles and items.
+  int64_t total_cost = W.evals[0] + W.evals[1] + W.evals[2] + W.evals[3];
+  const int64_t max_cost =
+      std::max<int64_t>((int64_t)kTile * 8192, total_cost / std::max<int64_t>(1, (int64_t)grid_slots * 8));
+  std::vector<std::pair<int64_t, WorkItem>> items;
+  for (int tp = 0; tp < Pt; ++tp) {
+    const int eb = head[tp], ee = head[tp + 1];
+    if (eb == ee) continue;
+    const int e0 = (int)W.entries.size();
+    int s_total = 0;
+    for (int k = eb; k < ee; ++k)
+      if (grouped[k].s_count > 0) {
+        W.entries.push_back(grouped[k]);
+        s_total += grouped[k].s_count;
+      }
+    const int e1 = (int)W.entries.size();
+    if (s_total == 0) continue;
+    const bool proxy = !T.h.is_leaf[tp];
+    const int t0 = proxy ? nt + T.cluster_slot[tp] * ipc : T.leaf_begin[tp];
+    const int tn = proxy ? ipc : T.h.point_count[tp];
+    for (int a = 0; a < tn; a += kTile) {
+      const int tc = std::min(kTile, tn - a);
+      const int64_t cost = (int64_t)tc * s_total;
+      const int nsplit = (int)std::min<int64_t>((cost + max_cost - 1) / max_cost, e1 - e0);
+      if (nsplit <= 1) {
+        items.push_back({cost, WorkItem{t0 + a, tc, e0, e1, s_total, proxy ? kItemProxyTargets : 0, 0, 0}});
+        continue;
+      }
+      // Split the entry range into nsplit pieces of similar source counts.
+      const int64_t per = (s_total + nsplit - 1) / nsplit;
+      int k = e0;
+      while (k < e1) {
+        int kb = k, st = 0;
+        while (k < e1 && (st == 0 || st + W.entries[k].s_count <= per)) st += W.entries[k++].s_count;
+        items.push_back({(int64_t)tc * st, WorkItem{t0 + a, tc, kb, k, st,
+                                                     (proxy ? kItemProxyTargets : 0) | kItemAtomic, 0, 0}});
+      }
+    }
+  }
+  std::stable_sort(items.begin(), items.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  W.items.resize(items.size());
+  for (size_t i = 0; i < items.size(); ++i) W.items[i] = items[i].second;
+  return BTK_OK;
+}
+
+void kind_scales(int dim, int kind, double* sc) {
+  const double pi = 3.141592653589793238462643383279502884;
+  const double q4 = 1.0 / (4.0 * pi);
+  for (int c = 0; c < 4; ++c) sc[c] = 0.0;
+  if (dim == 2) {
+    sc[0] = q4;                                    // +(1/4pi) log(r^2+eps^2)
+    if (kind == BTK_KIND_FIELD) sc[1] = sc[2] = -1.0 / (2.0 * pi);
+  } else if (kind == BTK_KIND_VEL) {
+    sc[0] = sc[1] = sc[2] = -q4;                   // -(1/4pi) q (t-s)/(r^2+eps^2)
+  } else {
+    sc[0] = -q4;                                   // -(1/4pi)/sqrt(r^2+eps^2)
+    if (kind == BTK_KIND_FIELD) sc[1] = sc[2] = sc[3] = -q4;
+  }
+}
+
+// ---- the interaction phase on prepared device data ----------------------------
+struct InteractCtx {
+  int dim, kind, precision;
+  double eps;
+  WorkItem* d_items = nullptr;
+  Entry* d_entries = nullptr;
+  int n_items = 0;
+  int* d_ticket_status = nullptr;  // [0] ticket, [1] status
+};
+
+btk_status run_interactions(const InteractCtx& C, const double4* S4, const double4* T4, const int* T_out,
+                            Ptr4 out, Ptr4 ptw, cudaStream_t st) {
+  if (C.n_items == 0) return BTK_OK;
+  InteractParams p{};
+  p.items = C.d_items;
+  p.n_items = C.n_items;
+  p.entries = C.d_entries;
+  p.S4 = S4;
+  p.T4 = T4;
+  p.T_out = T_out;
+  for (int c = 0; c < 4; ++c) {
+    p.out[c] = out.p[c];
+    p.ptw[c] = ptw.p[c];
+  }
+  p.eps2 = C.eps * C.eps;
+  kind_scales(C.dim, C.kind, p.scale);
+  p.ticket = C.d_ticket_status;
+  p.status = C.d_ticket_status + 1;
+  const bool guard = p.eps2 < 1.1754943508222875e-38;
+  int per_sm = interact_blocks_per_sm(C.dim, C.kind, C.precision, guard);
+  if (per_sm <= 0) per_sm = 1;
+  const int grid = std::min(C.n_items, num_sms() * per_sm);
+  BTK_CUDA(cudaMemsetAsync(C.d_ticket_status, 0, sizeof(int), st));
+  BTK_CUDA(launch_interact(C.dim, C.kind, C.precision, guard, p, grid, st));
+  return BTK_OK;
+}
+
+btk_status validate_cfg(const btk_run_config* cfg, int dim) {
+  BTK_CHECK(cfg, BTK_ERR_INVALID_ARGUMENT, "null run config");
+  BTK_CHECK(cfg->dim == dim, BTK_ERR_INVALID_ARGUMENT, "run config dim does not match the entry point");
+  BTK_CHECK(cfg->interp_degree >= 1 && cfg->interp_degree <= kMaxDegree, BTK_ERR_UNSUPPORTED,
+            "interp_degree outside 1..12");
+  BTK_CHECK(cfg->interp_point_count == ipow(cfg->interp_degree + 1, dim), BTK_ERR_INVALID_ARGUMENT,
+            "interp_point_count != (interp_degree+1)^dim");
+  BTK_CHECK(cfg->fmm_cluster_thresh > 0, BTK_ERR_INVALID_ARGUMENT, "fmm_cluster_thresh must be positive");
+  BTK_CHECK(std::isfinite(cfg->ker_eps), BTK_ERR_INVALID_ARGUMENT, "ker_eps must be finite");
+  return BTK_OK;
+}
+
+template <class P>
+btk_status fetch_panels(const P* d_panels, int count, std::vector<P>& host, cudaStream_t st) {
+  BTK_CHECK(d_panels || count == 0, BTK_ERR_INVALID_ARGUMENT, "null panel array");
+  BTK_CHECK(count > 0, BTK_ERR_INVALID_ARGUMENT, "panel count must be positive");
+  host.resize(count);
+  BTK_CUDA(cudaMemcpyAsync(host.data(), d_panels, sizeof(P) * count, cudaMemcpyDeviceToHost, st));
+  return BTK_OK;
+}
+
+template <class T>
+btk_status fetch(const T* d, int count, std::vector<T>& host, cudaStream_t st) {
+  host.resize(count);
+  if (count == 0) return BTK_OK;
+  BTK_CHECK(d, BTK_ERR_INVALID_ARGUMENT, "null device array");
+  BTK_CUDA(cudaMemcpyAsync(host.data(), d, sizeof(T) * count, cudaMemcpyDeviceToHost, st));
+  return BTK_OK;
+}
+
+btk_status check_status_word(const int* d_status, cudaStream_t st) {
+  int h = 0;
+  BTK_CUDA(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  if (h != 0) return set_error((btk_status)h, "device-side wait timed out in the interaction kernel");
+  return BTK_OK;
+}
+
+}  // namespace
+}  // namespace btk
+
+// =============================================================================
+// Plan API
+// =============================================================================
+struct btk_plan {
+  int dim = 3, degree = 8, m = 9, ipc = 729, kind = 0, precision = 0, ncomp = 1, thresh = 0;
+  double eps = 0;
+  bool same_tree = true;
+  cudaStream_t stream = nullptr;
+  std::unique_ptr<btk::Arena> arena;
+  btk::Side tgt, src_own;
+  btk::Side* src = nullptr;
+  btk::InteractCtx ictx;
+  int64_t evals[4] = {0, 0, 0, 0};
+  // device work arrays
+  double4 *d_S4 = nullptr, *d_T4 = nullptr;
+  int* d_T_out = nullptr;
+  double* d_psw = nullptr;
+  double* d_ptw = nullptr;  // ncomp x Pt x ipc
+  int* d_ticket_status = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool timed = false;
+};
+
+using namespace btk;
+
+namespace {
+
+btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
+  const btk_run_config& cfg = D->cfg;
+  BTK_CHECK(cfg.dim == 2 || cfg.dim == 3, BTK_ERR_INVALID_ARGUMENT, "dim must be 2 or 3");
+  BTK_TRY(validate_cfg(&cfg, cfg.dim));
+  BTK_CHECK(D->kind >= 0 && D->kind <= 2, BTK_ERR_INVALID_ARGUMENT, "bad kind");
+  BTK_CHECK(!(D->kind == BTK_KIND_VEL && cfg.dim != 3), BTK_ERR_UNSUPPORTED, "VEL kernel is 3-D only");
+  BTK_CHECK(D->precision == BTK_PREC_FP64, BTK_ERR_UNSUPPORTED, "precision not available in this build");
+  BTK_CHECK(D->tree_target && D->panels_target && D->panel_points_inside_target && D->point_leaf_panel_source,
+            BTK_ERR_INVALID_ARGUMENT, "plan: missing tree arrays");
+  P->dim = cfg.dim;
+  P->degree = cfg.interp_degree;
+  P->m = P->degree + 1;
+  P->ipc = cfg.interp_point_count;
+  P->kind = D->kind;
+  P->precision = D->precision;
+  P->ncomp = ncomp_of(cfg.dim, D->kind);
+  P->thresh = cfg.fmm_cluster_thresh;
+  P->eps = cfg.ker_eps;
+  P->stream = st;
+  P->same_tree = D->panels_source == nullptr;
+  P->arena.reset(new Arena(st));
+  Arena& A = *P->arena;
+
+  host_tree_from_panels(cfg.dim, D->panels_target, D->tree_target->panel_count, D->tree_target->level_start,
+                        D->tree_target->levels, P->tgt.h);
+  BTK_TRY(side_layout(P->tgt, D->point_count_target, P->degree));
+  BTK_TRY(side_upload(P->tgt, A, D->panel_points_inside_target, nullptr, P->thresh));
+  if (P->same_tree) {
+    P->src = &P->tgt;
+    BTK_CHECK(D->point_count_source == D->point_count_target, BTK_ERR_INVALID_ARGUMENT,
+              "one tree but different point counts");
+  } else {
+    BTK_CHECK(D->tree_source && D->panel_points_inside_source, BTK_ERR_INVALID_ARGUMENT, "plan: missing source tree");
+    host_tree_from_panels(cfg.dim, D->panels_source, D->tree_source->panel_count, D->tree_source->level_start,
+                          D->tree_source->levels, P->src_own.h);
+    BTK_TRY(side_layout(P->src_own, D->point_count_source, P->degree));
+    BTK_TRY(side_upload(P->src_own, A, D->panel_points_inside_source, nullptr, P->thresh));
+    P->src = &P->src_own;
+  }
+  Side& T = P->tgt;
+  Side& S = *P->src;
+  const int nct = (int)T.clusters.size(), ncs = (int)S.clusters.size();
+  const int Pt = T.h.panel_count, Ps = S.h.panel_count;
+
+  // Work lists.
+  const btk_interact_pair* lists[4] = {D->pp_list, D->pc_list, D->cp_list, D->cc_list};
+  const int counts[4] = {cfg.fmm_pp_count, cfg.fmm_pc_count, cfg.fmm_cp_count, cfg.fmm_cc_count};
+  for (int t = 0; t < 4; ++t) BTK_CHECK(counts[t] >= 0 && (counts[t] == 0 || lists[t]), BTK_ERR_INVALID_ARGUMENT,
+                                        "plan: missing interaction list");
+  const bool guard = P->eps * P->eps < 1.1754943508222875e-38;
+  const int slots = num_sms() * std::max(1, interact_blocks_per_sm(P->dim, P->kind, P->precision, guard));
+  WorkLists W;
+  BTK_TRY(build_work(T, S, lists, counts, slots, W));
+  for (int t = 0; t < 4; ++t) P->evals[t] = W.evals[t];
+  P->ictx.dim = P->dim;
+  P->ictx.kind = P->kind;
+  P->ictx.precision = P->precision;
+  P->ictx.eps = P->eps;
+  P->ictx.n_items = (int)W.items.size();
+  BTK_TRY(A.upload(&P->ictx.d_items, W.items));
+  BTK_TRY(A.upload(&P->ictx.d_entries, W.entries));
+  BTK_TRY(A.alloc(&P->d_ticket_status, 2));
+  BTK_CUDA(cudaMemsetAsync(P->d_ticket_status, 0, 2 * sizeof(int), st));
+  P->ictx.d_ticket_status = P->d_ticket_status;
+
+  // Work arrays.
+  BTK_TRY(A.alloc(&P->d_S4, (size_t)S.n_points + (size_t)ncs * P->ipc));
+  BTK_TRY(A.alloc(&P->d_T4, (size_t)T.n_points + (size_t)nct * P->ipc));
+  BTK_TRY(A.alloc(&P->d_T_out, (size_t)T.n_points + (size_t)nct * P->ipc));
+  BTK_TRY(A.alloc(&P->d_psw, (size_t)Ps * P->ipc));
+  BTK_TRY(A.alloc(&P->d_ptw, (size_t)P->ncomp * Pt * P->ipc));
+  if (T.n_points)
+    BTK_CUDA(cudaMemcpyAsync(P->d_T_out, T.d_perm, sizeof(int) * T.n_points, cudaMemcpyDeviceToDevice, st));
+  BTK_CUDA(launch_tgt_proxies(P->dim, P->degree, nct, T.d_clusters, T.d_nodes_shift, P->d_T4 + T.n_points,
+                              P->d_T_out + T.n_points, st));
+  for (int i = 0; i < 4; ++i) BTK_CUDA(cudaEventCreate(&P->ev[i]));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  return BTK_OK;
+}
+
+// Upward pass on a side whose sorted points (S4 prefix) are in place.
+btk_status run_upward(const Side& S, const double4* pts, double* psw, cudaStream_t st) {
+  BTK_CUDA(launch_leaf_moments(S.h.dim, S.degree, (int)S.leaves.size(), S.d_leaves, S.d_leaf_begin, S.d_point_count,
+                               pts, S.d_nodes_interp, psw, st));
+  for (int l = S.h.levels - 2; l >= 0; --l)
+    BTK_CUDA(launch_c2p(S.h.dim, S.degree, (int)S.nonleaf_by_level[l].size(), S.d_nonleaf_by_level[l], S.d_child,
+                        S.d_xfer, psw, st));
+  return BTK_OK;
+}
+
+btk_status run_downward(const Side& T, int ncomp, const double4* pts, Ptr4 ptw, Ptr4 out, cudaStream_t st) {
+  for (int l = 1; l < T.h.levels; ++l)
+    BTK_CUDA(launch_p2c(T.h.dim, T.degree, ncomp, (int)T.panels_by_level[l].size(), T.d_panels_by_level[l],
+                        T.d_parent, T.d_xfer, ptw, T.ipc, st));
+  BTK_CUDA(launch_l2p(T.h.dim, T.degree, ncomp, (int)T.leaves.size(), T.d_leaves, T.d_leaf_begin, T.d_point_count,
+                      pts, T.d_perm, T.d_nodes_interp, ptw, out, st));
+  return BTK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+btk_status btk_plan_create(btk_plan** plan, const btk_plan_desc* desc, btk_stream_t stream) {
+  BTK_CHECK(plan && desc, BTK_ERR_INVALID_ARGUMENT, "btk_plan_create: null argument");
+  *plan = nullptr;
+  btk_plan* P = new btk_plan();
+  btk_status s = plan_build(P, desc, (cudaStream_t)stream);
+  if (s != BTK_OK) {
+    btk_plan_destroy(P);
+    return s;
+  }
+  *plan = P;
+  return BTK_OK;
+}
+
+btk_status btk_plan_destroy(btk_plan* plan) {
+  if (!plan) return BTK_OK;
+  cudaDeviceSynchronize();
+  for (auto& e : plan->ev)
+    if (e) cudaEventDestroy(e);
+  plan->arena.reset();
+  cudaStreamSynchronize(plan->stream);
+  delete plan;
+  return BTK_OK;
+}
+
+btk_status btk_plan_stats_get(const btk_plan* plan, btk_plan_stats* st) {
+  BTK_CHECK(plan && st, BTK_ERR_INVALID_ARGUMENT, "null argument");
+  st->evals_pp = plan->evals[0];
+  st->evals_pc = plan->evals[1];
+  st->evals_cp = plan->evals[2];
+  st->evals_cc = plan->evals[3];
+  st->work_items = plan->ictx.n_items;
+  st->device_bytes = (int64_t)plan->arena->bytes;
+  st->levels_target = plan->tgt.h.levels;
+  st->levels_source = plan->src->h.levels;
+  return BTK_OK;
+}
+
+btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, const double* zt, const double* xs,
+                            const double* ys, const double* zs, const double* charges, double* out,
+                            btk_stream_t stream) {
+  BTK_CHECK(P && xt && yt && xs && ys && charges && out, BTK_ERR_INVALID_ARGUMENT, "btk_plan_execute: null argument");
+  BTK_CHECK(P->dim == 2 || (zt && zs), BTK_ERR_INVALID_ARGUMENT, "btk_plan_execute: null z coordinates");
+  cudaStream_t st = (cudaStream_t)stream;
+  Side& T = P->tgt;
+  Side& S = *P->src;
+  const int Pt = T.h.panel_count;
+  BTK_CUDA(cudaEventRecord(P->ev[0], st));
+  // Upward.
+  BTK_CUDA(launch_gather(S.n_points, S.d_perm, xs, ys, P->dim == 3 ? zs : nullptr, charges, P->d_S4, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_psw, 0, sizeof(double) * (size_t)S.h.panel_count * P->ipc, st));
+  BTK_TRY(run_upward(S, P->d_S4, P->d_psw, st));
+  BTK_CUDA(launch_src_proxies(P->dim, P->degree, (int)S.clusters.size(), S.d_clusters, S.d_nodes_shift, P->d_psw,
+                              P->d_S4 + S.n_points, st));
+  BTK_CUDA(cudaEventRecord(P->ev[1], st));
+  // Interactions.
+  BTK_CUDA(launch_gather(T.n_points, T.d_perm, xt, yt, P->dim == 3 ? zt : nullptr, nullptr, P->d_T4, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_ptw, 0, sizeof(double) * (size_t)P->ncomp * Pt * P->ipc, st));
+  BTK_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)P->ncomp * T.n_points, st));
+  Ptr4 o{}, w{};
+  for (int c = 0; c < P->ncomp; ++c) {
+    o.p[c] = out + (size_t)c * T.n_points;
+    w.p[c] = P->d_ptw + (size_t)c * Pt * P->ipc;
+  }
+  BTK_TRY(run_interactions(P->ictx, P->d_S4, P->d_T4, P->d_T_out, o, w, st));
+  BTK_CUDA(cudaEventRecord(P->ev[2], st));
+  // Downward.
+  BTK_TRY(run_downward(T, P->ncomp, P->d_T4, w, o, st));
+  BTK_CUDA(cudaEventRecord(P->ev[3], st));
+  P->timed = true;
+  return BTK_OK;
+}
+
+btk_status btk_plan_last_timing(btk_plan* P, float* ms) {
+  BTK_CHECK(P && ms, BTK_ERR_INVALID_ARGUMENT, "null argument");
+  BTK_CHECK(P->timed, BTK_ERR_INVALID_ARGUMENT, "plan has not executed");
+  BTK_CUDA(cudaEventSynchronize(P->ev[3]));
+  BTK_CUDA(cudaEventElapsedTime(&ms[0], P->ev[0], P->ev[1]));
+  BTK_CUDA(cudaEventElapsedTime(&ms[1], P->ev[1], P->ev[2]));
+  BTK_CUDA(cudaEventElapsedTime(&ms[2], P->ev[2], P->ev[3]));
+  BTK_CUDA(cudaEventElapsedTime(&ms[3], P->ev[0], P->ev[3]));
+  return check_status_word(P->d_ticket_status + 1, P->stream);
+}
+
+btk_status btk_solve_host(int dim, int kind, int precision, int degree, int cluster_size, double theta, double eps,
+                          int n, const double* x, const double* y, const double* z, const double* charges,
+                          double* out, btk_stream_t stream) {
+  BTK_CHECK(dim == 2 || dim == 3, BTK_ERR_INVALID_ARGUMENT, "dim must be 2 or 3");
+  BTK_CHECK(n > 0 && x && y && charges && out && (dim == 2 || z), BTK_ERR_INVALID_ARGUMENT,
+            "btk_solve_host: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  btk_run_config cfg{};
+  cfg.dim = dim;
+  cfg.interp_degree = degree;
+  cfg.interp_point_count = ipow(degree + 1, dim);
+  cfg.fmm_cluster_thresh = cluster_size > 0 ? cluster_size : (1 << dim) * cfg.interp_point_count;
+  cfg.fmm_theta = theta;
+  cfg.ker_eps = eps;
+  cfg.mpi_p = 1;
+  btk_tree_info info{};
+  void* panels = nullptr;
+  int* inside = nullptr;
+  std::vector<int> leaf_of(n);
+  btk_status s = dim == 2 ? btk_tree_construction_2d(&cfg, &info, x, y, n, (btk_panel_2d**)&panels, leaf_of.data(), &inside)
+                          : btk_tree_construction_3d(&cfg, &info, x, y, z, n, (btk_panel_3d**)&panels, leaf_of.data(), &inside);
+  if (s != BTK_OK) return s;
+  std::unique_ptr<void, void (*)(void*)> g1(panels, std::free), g2(inside, std::free), g3(info.level_start, std::free);
+  btk_interact_pair* all = nullptr;
+  s = dim == 2 ? btk_dual_tree_traversal_2d(&cfg, (btk_panel_2d*)panels, (btk_panel_2d*)panels, &all)
+               : btk_dual_tree_traversal_3d(&cfg, (btk_panel_3d*)panels, (btk_panel_3d*)panels, &all);
+  if (s != BTK_OK) return s;
+  std::unique_ptr<void, void (*)(void*)> g4(all, std::free);
+  std::vector<btk_interact_pair> L[4];
+  L[0].resize(cfg.fmm_pp_count);
+  L[1].resize(cfg.fmm_pc_count);
+  L[2].resize(cfg.fmm_cp_count);
+  L[3].resize(cfg.fmm_cc_count);
+  BTK_TRY(btk_split_interactions(all, cfg.fmm_interaction_count, L[0].data(), L[1].data(), L[2].data(), L[3].data()));
+  btk_plan_desc D{};
+  D.cfg = cfg;
+  D.point_count_target = D.point_count_source = n;
+  D.tree_target = &info;
+  D.panels_target = panels;
+  D.panel_points_inside_target = inside;
+  D.point_leaf_panel_source = leaf_of.data();
+  D.pp_list = L[0].data();
+  D.pc_list = L[1].data();
+  D.cp_list = L[2].data();
+  D.cc_list = L[3].data();
+  D.kind = kind;
+  D.precision = precision;
+  btk_plan* P = nullptr;
+  BTK_TRY(btk_plan_create(&P, &D, stream));
+  std::unique_ptr<btk_plan, btk_status (*)(btk_plan*)> gp(P, btk_plan_destroy);
+  const int nc = ncomp_of(dim, kind);
+  Arena A(st);
+  double *d_xyz = nullptr, *d_q = nullptr, *d_out = nullptr;
+  BTK_TRY(A.alloc(&d_xyz, (size_t)3 * n));
+  BTK_TRY(A.alloc(&d_q, (size_t)n));
+  BTK_TRY(A.alloc(&d_out, (size_t)nc * n));
+  BTK_CUDA(cudaMemcpyAsync(d_xyz, x, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  BTK_CUDA(cudaMemcpyAsync(d_xyz + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  if (dim == 3) BTK_CUDA(cudaMemcpyAsync(d_xyz + 2 * (size_t)n, z, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  BTK_CUDA(cudaMemcpyAsync(d_q, charges, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  const double* dz = dim == 3 ? d_xyz + 2 * (size_t)n : nullptr;
+  BTK_TRY(btk_plan_execute(P, d_xyz, d_xyz + n, dz, d_xyz, d_xyz + n, dz, d_q, d_out, stream));
+  BTK_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * nc * (size_t)n, cudaMemcpyDeviceToHost, st));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  return check_status_word(P->d_ticket_status + 1, st);
+}
+
+}  // extern "C"
+
+// =============================================================================
+// Drop-in entry points (reference names and argument order; device pointers)
+// =============================================================================
+
+static btk_status upward_dropin(int dim, const btk_run_config* cfg, const btk_tree_info* info, const double* x,
+                                const double* y, const double* z, const double* q, const void* d_panels, double* psw,
+                                const int* d_leaf_of, int n, cudaStream_t st) {
+  BTK_TRY(validate_cfg(cfg, dim));
+  BTK_CHECK(info && info->level_start && info->panel_count > 0 && info->levels > 0, BTK_ERR_INVALID_ARGUMENT,
+            "upward_pass: bad tree_info");
+  BTK_CHECK(n >= 0 && x && y && q && psw && d_leaf_of && (dim == 2 || z), BTK_ERR_INVALID_ARGUMENT,
+            "upward_pass: null argument");
+  Side S;
+  std::vector<int> leaf_of;
+  if (dim == 2) {
+    std::vector<btk_panel_2d> hp;
+    BTK_TRY(fetch_panels((const btk_panel_2d*)d_panels, info->panel_count, hp, st));
+    BTK_TRY(fetch(d_leaf_of, n, leaf_of, st));
+    BTK_CUDA(cudaStreamSynchronize(st));
+    host_tree_from_panels(2, hp.data(), info->panel_count, info->level_start, info->levels, S.h);
+  } else {
+    std::vector<btk_panel_3d> hp;
+    BTK_TRY(fetch_panels((const btk_panel_3d*)d_panels, info->panel_count, hp, st));
+    BTK_TRY(fetch(d_leaf_of, n, leaf_of, st));
+    BTK_CUDA(cudaStreamSynchronize(st));
+    host_tree_from_panels(3, hp.data(), info->panel_count, info->level_start, info->levels, S.h);
+  }
+  BTK_TRY(side_layout(S, n, cfg->interp_degree));
+  Arena A(st);
+  BTK_TRY(side_upload(S, A, nullptr, nullptr, cfg->fmm_cluster_thresh));
+  BTK_TRY(side_perm_from_leaf_of(S, A, leaf_of));
+  double4* pts = nullptr;
+  BTK_TRY(A.alloc(&pts, (size_t)std::max(n, 1)));
+  BTK_CUDA(launch_gather(n, S.d_perm, x, y, dim == 3 ? z : nullptr, q, pts, st));
+  BTK_TRY(run_upward(S, pts, psw, st));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  return BTK_OK;
+}
+
+template <class PanelT>
+static btk_status interactions_dropin(int dim, int kind, const btk_run_config* cfg, const double* xt, const double* yt,
+                                      const double* zt, const double* xs, const double* ys, const double* zs,
+                                      const double* q, Ptr4 out, const int* inside_s, const int* inside_t,
+                                      const double* psw, Ptr4 ptw, const btk_interact_pair* const dl[4],
+                                      const PanelT* panels_s, const PanelT* panels_t, int nt, int ns, int Pt, int Ps,
+                                      cudaStream_t st) {
+  BTK_TRY(validate_cfg(cfg, dim));
+  BTK_CHECK(nt >= 0 && ns >= 0 && xt && yt && xs && ys && q && psw && inside_s && inside_t && (dim == 2 || (zt && zs)),
+            BTK_ERR_INVALID_ARGUMENT, "interactions: null argument");
+  const int counts[4] = {cfg->fmm_pp_count, cfg->fmm_pc_count, cfg->fmm_cp_count, cfg->fmm_cc_count};
+  std::vector<PanelT> hpt, hps;
+  std::vector<btk_interact_pair> hl[4];
+  BTK_TRY(fetch_panels(panels_t, Pt, hpt, st));
+  BTK_TRY(fetch_panels(panels_s, Ps, hps, st));
+  for (int t = 0; t < 4; ++t) BTK_TRY(fetch(dl[t], counts[t], hl[t], st));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  Side T, Sown;
+  BTK_CHECK(host_tree_from_panels_nolevels(dim, hpt.data(), Pt, T.h), BTK_ERR_INVALID_ARGUMENT,
+            "target panels are not in level order");
+  BTK_TRY(side_layout(T, nt, cfg->interp_degree));
+  BTK_CHECK(host_tree_from_panels_nolevels(dim, hps.data(), Ps, Sown.h), BTK_ERR_INVALID_ARGUMENT,
+            "source panels are not in level order");
+  BTK_TRY(side_layout(Sown, ns, cfg->interp_degree));
+  Arena A(st);
+  BTK_TRY(side_upload(T, A, nullptr, inside_t, cfg->fmm_cluster_thresh));
+  BTK_TRY(side_upload(Sown, A, nullptr, inside_s, cfg->fmm_cluster_thresh));
+  const Side& S = Sown;
+  const int ipc = S.ipc;
+  const int nct = (int)T.clusters.size(), ncs = (int)S.clusters.size();
+  // Sources: sorted points + cluster proxies carrying the modified charges.
+  double4 *S4 = nullptr, *T4 = nullptr;
+  int* T_out = nullptr;
+  BTK_TRY(A.alloc(&S4, (size_t)ns + (size_t)ncs * ipc + 1));
+  BTK_TRY(A.alloc(&T4, (size_t)nt + (size_t)nct * ipc + 1));
+  BTK_TRY(A.alloc(&T_out, (size_t)nt + (size_t)nct * ipc + 1));
+  BTK_CUDA(launch_gather(ns, S.d_perm, xs, ys, dim == 3 ? zs : nullptr, q, S4, st));
+  BTK_CUDA(launch_src_proxies(dim, S.degree, ncs, S.d_clusters, S.d_nodes_shift, psw, S4 + ns, st));
+  BTK_CUDA(launch_gather(nt, T.d_perm, xt, yt, dim == 3 ? zt : nullptr, nullptr, T4, st));
+  if (nt) BTK_CUDA(cudaMemcpyAsync(T_out, T.d_perm, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
+  BTK_CUDA(launch_tgt_proxies(dim, T.degree, nct, T.d_clusters, T.d_nodes_shift, T4 + nt, T_out + nt, st));
+  const btk_interact_pair* hlp[4] = {hl[0].data(), hl[1].data(), hl[2].data(), hl[3].data()};
+  const bool guard = cfg->ker_eps * cfg->ker_eps < 1.1754943508222875e-38;
+  const int slots = num_sms() * std::max(1, interact_blocks_per_sm(dim, kind, BTK_PREC_FP64, guard));
+  WorkLists W;
+  BTK_TRY(build_work(T, S, hlp, counts, slots, W));
+  InteractCtx C;
+  C.dim = dim;
+  C.kind = kind;
+  C.precision = BTK_PREC_FP64;
+  C.eps = cfg->ker_eps;
+  C.n_items = (int)W.items.size();
+  BTK_TRY(A.upload(&C.d_items, W.items));
+  BTK_TRY(A.upload(&C.d_entries, W.entries));
+  BTK_TRY(A.alloc(&C.d_ticket_status, 2));
+  BTK_CUDA(cudaMemsetAsync(C.d_ticket_status, 0, 2 * sizeof(int), st));
+  BTK_TRY(run_interactions(C, S4, T4, T_out, out, ptw, st));
+  return check_status_word(C.d_ticket_status + 1, st);
+}
+
+template <class PanelT>
+static btk_status downward_dropin(int dim, int ncomp, const btk_run_config* cfg, const btk_tree_info* info,
+                                  const double* x, const double* y, const double* z, Ptr4 out, const PanelT* panels,
+                                  Ptr4 ptw, const int* inside, int n, cudaStream_t st) {
+  BTK_TRY(validate_cfg(cfg, dim));
+  BTK_CHECK(info && info->level_start && info->panel_count > 0 && info->levels > 0, BTK_ERR_INVALID_ARGUMENT,
+            "downward_pass: bad tree_info");
+  BTK_CHECK(n >= 0 && x && y && inside && (dim == 2 || z), BTK_ERR_INVALID_ARGUMENT, "downward_pass: null argument");
+  std::vector<PanelT> hp;
+  BTK_TRY(fetch_panels(panels, info->panel_count, hp, st));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  Side T;
+  host_tree_from_panels(dim, hp.data(), info->panel_count, info->level_start, info->levels, T.h);
+  BTK_TRY(side_layout(T, n, cfg->interp_degree));
+  Arena A(st);
+  BTK_TRY(side_upload(T, A, nullptr, inside, cfg->fmm_cluster_thresh));
+  double4* pts = nullptr;
+  BTK_TRY(A.alloc(&pts, (size_t)std::max(n, 1)));
+  BTK_CUDA(launch_gather(n, T.d_perm, x, y, dim == 3 ? z : nullptr, nullptr, pts, st));
+  BTK_TRY(run_downward(T, ncomp, pts, ptw, out, st));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  return BTK_OK;
+}
+
+extern "C" {
+
+btk_status btk_upward_pass_2d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                              const double* ycos, const double* charges, const btk_panel_2d* blfmm_panels,
+                              double* proxy_source_weights, const int* point_leaf_panel, int point_count,
+                              btk_stream_t stream) {
+  return upward_dropin(2, cfg, info, xcos, ycos, nullptr, charges, blfmm_panels, proxy_source_weights,
+                       point_leaf_panel, point_count, (cudaStream_t)stream);
+}
+
+btk_status btk_upward_pass_3d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                              const double* ycos, const double* zcos, const double* charges,
+                              const btk_panel_3d* blfmm_panels, double* proxy_source_weights,
+                              const int* point_leaf_panel, int point_count, btk_stream_t stream) {
+  return upward_dropin(3, cfg, info, xcos, ycos, zcos, charges, blfmm_panels, proxy_source_weights, point_leaf_panel,
+                       point_count, (cudaStream_t)stream);
+}
+
+btk_status btk_poisson_fmm_interactions_2d(const btk_run_config* cfg, const double* xcos_t, const double* ycos_t,
+                                           const double* xcos_s, const double* ycos_s, const double* charges,
+                                           double* soln, const int* panel_points_inside_source,
+                                           const int* panel_points_inside_target, const double* proxy_source_weights,
+                                           double* proxy_target_weights, const btk_interact_pair* pp_ints,
+                                           const btk_interact_pair* pc_ints, const btk_interact_pair* cp_ints,
+                                           const btk_interact_pair* cc_ints, const btk_panel_2d* blfmm_panels_source,
+                                           const btk_panel_2d* blfmm_panels_target, int point_count_target,
+                                           int point_count_source, int panel_count_target, int panel_count_source,
+                                           btk_stream_t stream) {
+  BTK_CHECK(soln && proxy_target_weights, BTK_ERR_INVALID_ARGUMENT, "interactions: null output");
+  Ptr4 o{{soln}}, w{{proxy_target_weights}};
+  const btk_interact_pair* dl[4] = {pp_ints, pc_ints, cp_ints, cc_ints};
+  return interactions_dropin(2, BTK_KIND_POT, cfg, xcos_t, ycos_t, nullptr, xcos_s, ycos_s, nullptr, charges, o,
+                             panel_points_inside_source, panel_points_inside_target, proxy_source_weights, w, dl,
+                             blfmm_panels_source, blfmm_panels_target, point_count_target, point_count_source,
+                             panel_count_target, panel_count_source, (cudaStream_t)stream);
+}
+
+btk_status btk_poisson_fmm_interactions_3d(const btk_run_config* cfg, const double* xcos_t, const double* ycos_t,
+                                           const double* zcos_t, const double* xcos_s, const double* ycos_s,
+                                           const double* zcos_s, const double* charges, double* soln,
+                                           const int* panel_points_inside_source,
+                                           const int* panel_points_inside_target, const double* proxy_source_weights,
+                                           double* proxy_target_weights, const btk_interact_pair* pp_ints,
+                                           const btk_interact_pair* pc_ints, const btk_interact_pair* cp_ints,
+                                           const btk_interact_pair* cc_ints, const btk_panel_3d* blfmm_panels_source,
+                                           const btk_panel_3d* blfmm_panels_target, int point_count_target,
+                                           int point_count_source, int panel_count_target, int panel_count_source,
+                                           btk_stream_t stream) {
+  BTK_CHECK(soln && proxy_target_weights, BTK_ERR_INVALID_ARGUMENT, "interactions: null output");
+  Ptr4 o{{soln}}, w{{proxy_target_weights}};
+  const btk_interact_pair* dl[4] = {pp_ints, pc_ints, cp_ints, cc_ints};
+  return interactions_dropin(3, BTK_KIND_POT, cfg, xcos_t, ycos_t, zcos_t, xcos_s, ycos_s, zcos_s, charges, o,
+                             panel_points_inside_source, panel_points_inside_target, proxy_source_weights, w, dl,
+                             blfmm_panels_source, blfmm_panels_target, point_count_target, point_count_source,
+                             panel_count_target, panel_count_source, (cudaStream_t)stream);
+}
+
+btk_status btk_poisson_vel_fmm_interactions_3d(
+    const btk_run_config* cfg, const double* xcos_t, const double* ycos_t, const double* zcos_t, const double* xcos_s,
+    const double* ycos_s, const double* zcos_s, const double* charges, double* vel_x, double* vel_y, double* vel_z,
+    const int* panel_points_inside_source, const int* panel_points_inside_target, const double* proxy_source_weights,
+    double* proxy_target_weights_x, double* proxy_target_weights_y, double* proxy_target_weights_z,
+    const btk_interact_pair* pp_ints, const btk_interact_pair* pc_ints, const btk_interact_pair* cp_ints,
+    const btk_interact_pair* cc_ints, const btk_panel_3d* blfmm_panels_source, const btk_panel_3d* blfmm_panels_target,
+    int point_count_target, int point_count_source, int panel_count_target, int panel_count_source,
+    btk_stream_t stream) {
+  BTK_CHECK(vel_x && vel_y && vel_z && proxy_target_weights_x && proxy_target_weights_y && proxy_target_weights_z,
+            BTK_ERR_INVALID_ARGUMENT, "vel interactions: null output");
+  Ptr4 o{{vel_x, vel_y, vel_z}}, w{{proxy_target_weights_x, proxy_target_weights_y, proxy_target_weights_z}};
+  const btk_interact_pair* dl[4] = {pp_ints, pc_ints, cp_ints, cc_ints};
+  return interactions_dropin(3, BTK_KIND_VEL, cfg, xcos_t, ycos_t, zcos_t, xcos_s, ycos_s, zcos_s, charges, o,
+                             panel_points_inside_source, panel_points_inside_target, proxy_source_weights, w, dl,
+                             blfmm_panels_source, blfmm_panels_target, point_count_target, point_count_source,
+                             panel_count_target, panel_count_source, (cudaStream_t)stream);
+}
+
+btk_status btk_downward_pass_2d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                                const double* ycos, double* soln, const btk_panel_2d* blfmm_panels,
+                                double* proxy_target_weights, const int* panel_points_inside, int point_count,
+                                btk_stream_t stream) {
+  BTK_CHECK(soln && proxy_target_weights, BTK_ERR_INVALID_ARGUMENT, "downward_pass: null output");
+  Ptr4 o{{soln}}, w{{proxy_target_weights}};
+  return downward_dropin(2, 1, cfg, info, xcos, ycos, nullptr, o, blfmm_panels, w, panel_points_inside, point_count,
+                         (cudaStream_t)stream);
+}
+
+btk_status btk_downward_pass_3d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                                const double* ycos, const double* zcos, double* soln,
+                                const btk_panel_3d* blfmm_panels, double* proxy_target_weights,
+                                const int* panel_points_inside, int point_count, btk_stream_t stream) {
+  BTK_CHECK(soln && proxy_target_weights, BTK_ERR_INVALID_ARGUMENT, "downward_pass: null output");
+  Ptr4 o{{soln}}, w{{proxy_target_weights}};
+  return downward_dropin(3, 1, cfg, info, xcos, ycos, zcos, o, blfmm_panels, w, panel_points_inside, point_count,
+                         (cudaStream_t)stream);
+}
+
+btk_status btk_downward_pass_3d_3(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                                  const double* ycos, const double* zcos, double* vel_x, double* vel_y, double* vel_z,
+                                  const btk_panel_3d* blfmm_panels, double* proxy_target_weights_x,
+                                  double* proxy_target_weights_y, double* proxy_target_weights_z,
+                                  const int* panel_points_inside, int point_count, btk_stream_t stream) {
+  BTK_CHECK(vel_x && vel_y && vel_z && proxy_target_weights_x && proxy_target_weights_y && proxy_target_weights_z,
+            BTK_ERR_INVALID_ARGUMENT, "downward_pass_3d_3: null output");
+  Ptr4 o{{vel_x, vel_y, vel_z}}, w{{proxy_target_weights_x, proxy_target_weights_y, proxy_target_weights_z}};
+  return downward_dropin(3, 3, cfg, info, xcos, ycos, zcos, o, blfmm_panels, w, panel_points_inside, point_count,
+                         (cudaStream_t)stream);
+}
+
+btk_status btk_direct_sum(int dim, int kind, double eps, int nt, const double* xt, const double* yt, const double* zt,
+                          int ns, const double* xs, const double* ys, const double* zs, const double* charges,
+                          double* out, btk_stream_t stream) {
+  BTK_CHECK(dim == 2 || dim == 3, BTK_ERR_INVALID_ARGUMENT, "dim must be 2 or 3");
+  BTK_CHECK(!(kind == BTK_KIND_VEL && dim != 3) && kind >= 0 && kind <= 2, BTK_ERR_INVALID_ARGUMENT, "bad kind");
+  BTK_CHECK(nt >= 0 && ns >= 0 && xt && yt && xs && ys && charges && out && (dim == 2 || (zt && zs)),
+            BTK_ERR_INVALID_ARGUMENT, "direct_sum: null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  Arena A(st);
+  double4* src = nullptr;
+  int* iota = nullptr;
+  BTK_TRY(A.alloc(&src, (size_t)std::max(ns, 1)));
+  std::vector<int> id(ns);
+  std::iota(id.begin(), id.end(), 0);
+  BTK_TRY(A.upload(&iota, id));
+  BTK_CUDA(launch_gather(ns, iota, xs, ys, dim == 3 ? zs : nullptr, charges, src, st));
+  BTK_CUDA(launch_direct(dim, kind, eps, nt, xt, yt, dim == 3 ? zt : nullptr, ns, src, out, st));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  return BTK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,309 @@
+/*
+ * barytreek_b200 — B200-native evaluation path of BarytreeK's barycentric
+ * Lagrange dual-tree treecode, exposed as a plain C ABI.
+ *
+ * Three layers, all extern "C", no torch or Kokkos types:
+ *
+ *  1. Host tree functions, bit-identical to the reference's host C++
+ *     (read_run_config, blfmm_tree_construction_2d/3d, dual_tree_traversal_2d/3d,
+ *     split_interactions). Outputs the reference's struct layouts.
+ *  2. Drop-in device entry points with the reference's names and argument
+ *     order (upward_pass_*, poisson_fmm_interactions_*,
+ *     poisson_vel_fmm_interactions_3d, downward_pass_*). Every array argument is
+ *     a DEVICE pointer laid out like the corresponding Kokkos::View
+ *     (LayoutRight, row = panel); extents a View would carry are appended
+ *     before the stream. Results accumulate (+=) like the reference's
+ *     atomic_add; proxy arrays must be zeroed by the caller as the reference's
+ *     drivers do (examples/example_poisson_3d.cpp:133-135).
+ *  3. A plan API (btk_plan_*) that keeps the tree, the target-grouped work
+ *     lists and all derived device data resident across solves, adds the
+ *     extensions (field/gradient outputs, mixed precision) and a one-call
+ *     host-buffer solve (btk_solve_host).
+ *
+ * Every function returns btk_status (0 = success); btk_last_error() gives a
+ * thread-local message for the last failure on the calling thread. Launches are
+ * asynchronous on the given stream unless stated otherwise.
+ */
+#ifndef BARYTREEK_B200_H
+#define BARYTREEK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same handle type as cudaStream_t (a CUstream); NULL = legacy default stream. */
+typedef struct CUstream_st* btk_stream_t;
+
+typedef enum {
+  BTK_OK = 0,
+  BTK_ERR_INVALID_ARGUMENT = 1,
+  BTK_ERR_CUDA = 2,
+  BTK_ERR_UNSUPPORTED = 3,
+  BTK_ERR_OUT_OF_MEMORY = 4,
+  BTK_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait gave up */
+  BTK_ERR_IO = 6,
+  BTK_ERR_INTERNAL = 7
+} btk_status;
+
+/* ---- Reference layouts (src/structs.hpp:6-75), byte-for-byte ---------- */
+
+/* RunConfig, src/structs.hpp:6-22 (64 bytes). */
+typedef struct {
+  int dim;
+  int interp_degree;
+  int interp_point_count;
+  double fmm_theta;
+  int fmm_cluster_thresh;
+  int fmm_interaction_count;
+  int fmm_pp_count;
+  int fmm_pc_count;
+  int fmm_cp_count;
+  int fmm_cc_count;
+  double ker_eps;
+  int mpi_p;
+  int mpi_id;
+} btk_run_config;
+
+/* TreeInfo, src/structs.hpp:24-28 (16 bytes). level_start has levels+1
+ * entries and lives in HOST memory (the reference's upward/downward loops read
+ * it on the host: src/upward_pass.cpp:12-16). */
+typedef struct {
+  int panel_count;
+  int levels;
+  int* level_start;
+} btk_tree_info;
+
+/* TreePanel_2d, src/structs.hpp:30-45 (80 bytes). */
+typedef struct {
+  int id, level, parent_id;
+  int child1, child2, child3, child4;
+  bool is_leaf;
+  double max_x, min_x, max_y, min_y;
+  double radius;
+  int point_count;
+} btk_panel_2d;
+
+/* TreePanel_3d, src/structs.hpp:47-66 (112 bytes; min_z precedes max_z). */
+typedef struct {
+  int id, level, parent_id;
+  int child1, child2, child3, child4, child5, child6, child7, child8;
+  bool is_leaf;
+  double max_x, min_x, max_y, min_y, min_z, max_z;
+  double radius;
+  int point_count;
+} btk_panel_3d;
+
+/* interact_pair, src/structs.hpp:71-75 (12 bytes). type 0 pp, 1 pc, 2 cp, 3 cc. */
+typedef struct {
+  int target_panel;
+  int source_panel;
+  int interact_type;
+} btk_interact_pair;
+
+/* ---- Library ---------------------------------------------------------- */
+
+const char* btk_last_error(void);
+const char* btk_version(void);
+/* Number of CUDA kernels this library has launched in this process. */
+uint64_t btk_launch_count(void);
+/* Highest polynomial degree the device kernels accept. */
+int btk_max_degree(void);
+void btk_free(void* p); /* frees arrays the host tree functions allocate */
+
+/* ---- 1. Host tree functions (bit-identical to the reference) ----------- */
+
+/* src/read_namelist.cpp:10-43. cfg->dim must be set first, as the reference's
+ * drivers do. Parsing stops at the first unknown key. BTK_ERR_IO when the file
+ * cannot be opened (the reference throws "namelist not found"). The degree is
+ * clamped to 10, the reference's max_degree (barytreek-config.h.in:20). */
+btk_status btk_read_run_config(const char* file_name, btk_run_config* cfg);
+
+/* src/tree_construction.cpp:5-129 / :131-306. Inputs are host arrays of
+ * point_count coordinates. Outputs, allocated by the library (btk_free):
+ * *panels (info->panel_count records), info->level_start (levels+1 ints),
+ * *panel_points_inside (panel_count x cfg->fmm_cluster_thresh ints, row-major;
+ * rows of non-leaf panels are zero). point_leaf_panel[point_count] is caller
+ * storage. */
+btk_status btk_tree_construction_2d(const btk_run_config* cfg, btk_tree_info* info, const double* xcos,
+                                    const double* ycos, int point_count, btk_panel_2d** panels,
+                                    int* point_leaf_panel, int** panel_points_inside);
+btk_status btk_tree_construction_3d(const btk_run_config* cfg, btk_tree_info* info, const double* xcos,
+                                    const double* ycos, const double* zcos, int point_count, btk_panel_3d** panels,
+                                    int* point_leaf_panel, int** panel_points_inside);
+
+/* src/interaction_list.cpp:5-117 / :119-250. Updates cfg's interaction
+ * counts; *interaction_list (cfg->fmm_interaction_count pairs) is allocated
+ * by the library (btk_free). */
+btk_status btk_dual_tree_traversal_2d(btk_run_config* cfg, const btk_panel_2d* panels_target,
+                                      const btk_panel_2d* panels_source, btk_interact_pair** interaction_list);
+btk_status btk_dual_tree_traversal_3d(btk_run_config* cfg, const btk_panel_3d* panels_target,
+                                      const btk_panel_3d* panels_source, btk_interact_pair** interaction_list);
+
+/* src/interaction_list.cpp:252-277. Output arrays are caller storage sized by
+ * the counts in the traversal's config. */
+btk_status btk_split_interactions(const btk_interact_pair* interaction_list, int interaction_count,
+                                  btk_interact_pair* pp_list, btk_interact_pair* pc_list, btk_interact_pair* cp_list,
+                                  btk_interact_pair* cc_list);
+
+/* ---- 2. Drop-in device entry points (reference names and argument order) --
+ *
+ * Differences from the reference, by design:
+ *  - parent-to-child runs only from non-leaf panels and leaf-to-point runs on
+ *    every leaf (the reference skips leaves above the last level and reads
+ *    child index -1 for them: src/downward_pass.cpp:9-16);
+ *  - each call synchronises `stream` once to read the (small) panel and list
+ *    metadata into host memory for planning; point data stays on the device;
+ *  - degrees above btk_max_degree() are rejected (the reference clamps the
+ *    namelist value to 10 before any call). */
+
+/* src/upward_pass.hpp:7 */
+btk_status btk_upward_pass_2d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                              const double* ycos, const double* charges, const btk_panel_2d* blfmm_panels,
+                              double* proxy_source_weights, const int* point_leaf_panel, int point_count,
+                              btk_stream_t stream);
+/* src/upward_pass.hpp:9 */
+btk_status btk_upward_pass_3d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                              const double* ycos, const double* zcos, const double* charges,
+                              const btk_panel_3d* blfmm_panels, double* proxy_source_weights,
+                              const int* point_leaf_panel, int point_count, btk_stream_t stream);
+
+/* src/fmm_interactions/poisson_fmm.hpp:9-11 */
+btk_status btk_poisson_fmm_interactions_2d(const btk_run_config* cfg, const double* xcos_t, const double* ycos_t,
+                                           const double* xcos_s, const double* ycos_s, const double* charges,
+                                           double* soln, const int* panel_points_inside_source,
+                                           const int* panel_points_inside_target, const double* proxy_source_weights,
+                                           double* proxy_target_weights, const btk_interact_pair* pp_ints,
+                                           const btk_interact_pair* pc_ints, const btk_interact_pair* cp_ints,
+                                           const btk_interact_pair* cc_ints, const btk_panel_2d* blfmm_panels_source,
+                                           const btk_panel_2d* blfmm_panels_target, int point_count_target,
+                                           int point_count_source, int panel_count_target, int panel_count_source,
+                                           btk_stream_t stream);
+/* src/fmm_interactions/poisson_fmm.hpp:13-15 */
+btk_status btk_poisson_fmm_interactions_3d(const btk_run_config* cfg, const double* xcos_t, const double* ycos_t,
+                                           const double* zcos_t, const double* xcos_s, const double* ycos_s,
+                                           const double* zcos_s, const double* charges, double* soln,
+                                           const int* panel_points_inside_source,
+                                           const int* panel_points_inside_target, const double* proxy_source_weights,
+                                           double* proxy_target_weights, const btk_interact_pair* pp_ints,
+                                           const btk_interact_pair* pc_ints, const btk_interact_pair* cp_ints,
+                                           const btk_interact_pair* cc_ints, const btk_panel_3d* blfmm_panels_source,
+                                           const btk_panel_3d* blfmm_panels_target, int point_count_target,
+                                           int point_count_source, int panel_count_target, int panel_count_source,
+                                           btk_stream_t stream);
+/* src/fmm_interactions/poisson_vel_fmm.hpp:9-11 */
+btk_status btk_poisson_vel_fmm_interactions_3d(
+    const btk_run_config* cfg, const double* xcos_t, const double* ycos_t, const double* zcos_t, const double* xcos_s,
+    const double* ycos_s, const double* zcos_s, const double* charges, double* vel_x, double* vel_y, double* vel_z,
+    const int* panel_points_inside_source, const int* panel_points_inside_target, const double* proxy_source_weights,
+    double* proxy_target_weights_x, double* proxy_target_weights_y, double* proxy_target_weights_z,
+    const btk_interact_pair* pp_ints, const btk_interact_pair* pc_ints, const btk_interact_pair* cp_ints,
+    const btk_interact_pair* cc_ints, const btk_panel_3d* blfmm_panels_source, const btk_panel_3d* blfmm_panels_target,
+    int point_count_target, int point_count_source, int panel_count_target, int panel_count_source,
+    btk_stream_t stream);
+
+/* src/downward_pass.hpp:7 */
+btk_status btk_downward_pass_2d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                                const double* ycos, double* soln, const btk_panel_2d* blfmm_panels,
+                                double* proxy_target_weights, const int* panel_points_inside, int point_count,
+                                btk_stream_t stream);
+/* src/downward_pass.hpp:9 */
+btk_status btk_downward_pass_3d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                                const double* ycos, const double* zcos, double* soln,
+                                const btk_panel_3d* blfmm_panels, double* proxy_target_weights,
+                                const int* panel_points_inside, int point_count, btk_stream_t stream);
+/* src/downward_pass.hpp:11 */
+btk_status btk_downward_pass_3d_3(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
+                                  const double* ycos, const double* zcos, double* vel_x, double* vel_y, double* vel_z,
+                                  const btk_panel_3d* blfmm_panels, double* proxy_target_weights_x,
+                                  double* proxy_target_weights_y, double* proxy_target_weights_z,
+                                  const int* panel_points_inside, int point_count, btk_stream_t stream);
+
+/* Direct sums (src/direct_sum_impl.hpp:9-94), FP64 on the device: every
+ * (target, source) pair, target == source included. out[ncomp][nt] is
+ * OVERWRITTEN (ncomp per kernel kind, below). Targets may be a subset. */
+btk_status btk_direct_sum(int dim, int kind, double eps, int nt, const double* xt, const double* yt,
+                          const double* zt, int ns, const double* xs, const double* ys, const double* zs,
+                          const double* charges, double* out, btk_stream_t stream);
+
+/* ---- 3. Plan API ------------------------------------------------------ */
+
+/* Kernel kinds. POT is the reference potential (2-D +(1/4pi)log(r^2+eps^2),
+ * 3-D -1/(4pi sqrt(r^2+eps^2))). VEL is the reference's 3-D "velocity"
+ * kernel -(1/4pi) q (t-s)/(r^2+eps^2) (poisson_vel_fmm_impl.hpp:81-84).
+ * FIELD is the potential plus the field -grad_t phi of the regularised
+ * potential (2-D -(1/2pi) q (t-s)/(r^2+eps^2), 3-D -(1/4pi) q (t-s)/(r^2+eps^2)^1.5);
+ * FIELD has no reference counterpart. Output components: POT 1, VEL 3,
+ * FIELD 1+dim (potential first). */
+typedef enum { BTK_KIND_POT = 0, BTK_KIND_VEL = 1, BTK_KIND_FIELD = 2 } btk_kind;
+
+/* Arithmetic of the interaction kernels. FP64 is the reference method.
+ * MIXED evaluates in FP32 on coordinates relative to each tile's FP64 centre
+ * and keeps compensated per-target sums, with FP64 interpolation weights,
+ * near-node branch, centres and final sums. */
+typedef enum { BTK_PREC_FP64 = 0, BTK_PREC_MIXED = 1 } btk_precision;
+
+typedef struct btk_plan btk_plan;
+
+/* Everything a plan is built from. Arrays are HOST memory and are copied;
+ * the source_* fields may be NULL for targets = sources (one tree). */
+typedef struct {
+  btk_run_config cfg; /* dim, degree, thresh, eps and the four counts */
+  int point_count_target, point_count_source;
+  const btk_tree_info* tree_target;
+  const btk_tree_info* tree_source; /* NULL: same tree */
+  const void* panels_target;        /* btk_panel_2d[] or btk_panel_3d[] */
+  const void* panels_source;        /* NULL: same tree */
+  const int* panel_points_inside_target;
+  const int* panel_points_inside_source; /* NULL: same tree */
+  const int* point_leaf_panel_source;
+  const btk_interact_pair* pp_list;
+  const btk_interact_pair* pc_list;
+  const btk_interact_pair* cp_list;
+  const btk_interact_pair* cc_list;
+  int kind;      /* btk_kind */
+  int precision; /* btk_precision */
+} btk_plan_desc;
+
+btk_status btk_plan_create(btk_plan** plan, const btk_plan_desc* desc, btk_stream_t stream);
+btk_status btk_plan_destroy(btk_plan* plan);
+
+/* Work and memory figures of a plan. */
+typedef struct {
+  int64_t evals_pp, evals_pc, evals_cp, evals_cc; /* kernel evaluations per class */
+  int64_t work_items;                             /* interaction work items */
+  int64_t device_bytes;                           /* device memory the plan holds */
+  int levels_target, levels_source;
+} btk_plan_stats;
+btk_status btk_plan_stats_get(const btk_plan* plan, btk_plan_stats* stats);
+
+/* One solve on device-resident inputs: gathers points and charges into leaf
+ * order, runs the upward pass, the interactions and the downward pass, and
+ * writes out[ncomp][point_count_target] (OVERWRITTEN, original point order).
+ * x/y/z_* and charges are device arrays in the caller's order; z may be NULL
+ * in 2-D; target pointers may equal source pointers. */
+btk_status btk_plan_execute(btk_plan* plan, const double* xt, const double* yt, const double* zt,
+                            const double* xs, const double* ys, const double* zs, const double* charges,
+                            double* out, btk_stream_t stream);
+
+/* Phase timing of the last btk_plan_execute on this plan (CUDA events; the
+ * call synchronises on them). ms[0] upward, [1] interactions, [2] downward,
+ * [3] total. */
+btk_status btk_plan_last_timing(btk_plan* plan, float* ms);
+
+/* One call from host buffers: builds the tree and lists with the host tree
+ * functions, creates a plan, copies inputs to the device, solves, copies
+ * out[ncomp][n] back (host) and destroys the plan. Sources = targets. */
+btk_status btk_solve_host(int dim, int kind, int precision, int degree, int cluster_size, double theta,
+                          double eps, int n, const double* x, const double* y, const double* z,
+                          const double* charges, double* out, btk_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
