@@ -391,11 +391,14 @@ btk_status btk_read_run_config(const char* file_name, btk_run_config* cfg) {
   std::ifstream f(file_name);
   if (f.fail()) return set_error(BTK_ERR_IO, std::string("namelist not found: ") + file_name);
   // Key/value lines until the first key that is not one of the four
-  // (read_namelist.cpp:19-42); "end" terminates by convention.
+  // (read_namelist.cpp:19-42); "end" terminates by convention. End of file
+  // also terminates: the reference re-parses its last line forever when the
+  // file ends without a newline and without a terminating key (a failed
+  // getline leaves `line` unchanged), which is not reproduced.
   std::string line, key, value;
   try {
     while (true) {
-      std::getline(f, line);
+      if (!std::getline(f, line)) return BTK_OK;
       std::stringstream ss(line);
       std::getline(ss, key, '=');
       std::getline(ss, value);
