@@ -104,6 +104,7 @@ SIGNATURES = {
     "btk_plan_execute": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_plan_last_timing": [_vp, _vp],
     "btk_solve_host": [_ci, _ci, _ci, _ci, _ci, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp],
+    "btk_measure_pipe_peak": [_ci, _vp, _vp],
 }
 _RESTYPES = {"btk_last_error": ctypes.c_char_p, "btk_version": ctypes.c_char_p, "btk_launch_count": ctypes.c_uint64,
              "btk_free": None}

@@ -23,7 +23,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.pat
 # Host tree code must evaluate every expression exactly as written (bit-identical
 # trees and lists): no contraction into fused multiply-adds.
 PER_FILE = {"host_tree.cpp": ["-Xcompiler", "-ffp-contract=off"]}
-SOURCES = ["host_tree.cpp", "plan.cu", "kernels_updown.cu", "kernels_interact.cu", "kernels_direct.cu"]
+SOURCES = ["host_tree.cpp", "plan.cu", "kernels_updown.cu", "kernels_interact.cu", "kernels_direct.cu",
+           "kernels_probe.cu"]
 HEADERS = ["btk_internal.h", "kernels.cuh", "device_math.cuh"]
 
 

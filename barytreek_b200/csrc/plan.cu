@@ -330,7 +330,7 @@ struct InteractCtx {
 };
 
 btk_status run_interactions(const InteractCtx& C, const double4* S4, const double4* T4, const int* T_out,
-                            Ptr4 out, Ptr4 ptw, cudaStream_t st) {
+                            Ptr4 out, Ptr4 ptw, cudaStream_t st, cudaEvent_t e0 = nullptr, cudaEvent_t e1 = nullptr) {
   if (C.n_items == 0) return BTK_OK;
   InteractParams p{};
   p.items = C.d_items;
@@ -352,7 +352,9 @@ btk_status run_interactions(const InteractCtx& C, const double4* S4, const doubl
   if (per_sm <= 0) per_sm = 1;
   const int grid = std::min(C.n_items, num_sms() * per_sm);
   BTK_CUDA(cudaMemsetAsync(C.d_ticket_status, 0, sizeof(int), st));
+  if (e0) BTK_CUDA(cudaEventRecord(e0, st));
   BTK_CUDA(launch_interact(C.dim, C.kind, C.precision, guard, p, grid, st));
+  if (e1) BTK_CUDA(cudaEventRecord(e1, st));
   return BTK_OK;
 }
 
@@ -416,7 +418,7 @@ struct btk_plan {
   double* d_psw = nullptr;
   double* d_ptw = nullptr;  // ncomp x Pt x ipc
   int* d_ticket_status = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool timed = false;
 };
 
@@ -499,7 +501,7 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
     BTK_CUDA(cudaMemcpyAsync(P->d_T_out, T.d_perm, sizeof(int) * T.n_points, cudaMemcpyDeviceToDevice, st));
   BTK_CUDA(launch_tgt_proxies(P->dim, P->degree, nct, T.d_clusters, T.d_nodes_shift, P->d_T4 + T.n_points,
                               P->d_T_out + T.n_points, st));
-  for (int i = 0; i < 4; ++i) BTK_CUDA(cudaEventCreate(&P->ev[i]));
+  for (int i = 0; i < 6; ++i) BTK_CUDA(cudaEventCreate(&P->ev[i]));
   BTK_CUDA(cudaStreamSynchronize(st));
   return BTK_OK;
 }
@@ -590,7 +592,10 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
     o.p[c] = out + (size_t)c * T.n_points;
     w.p[c] = P->d_ptw + (size_t)c * Pt * P->ipc;
   }
-  BTK_TRY(run_interactions(P->ictx, P->d_S4, P->d_T4, P->d_T_out, o, w, st));
+  // The kernel-tight pair is recorded only when there is a launch to bracket.
+  BTK_CUDA(cudaEventRecord(P->ev[4], st));
+  BTK_CUDA(cudaEventRecord(P->ev[5], st));
+  BTK_TRY(run_interactions(P->ictx, P->d_S4, P->d_T4, P->d_T_out, o, w, st, P->ev[4], P->ev[5]));
   BTK_CUDA(cudaEventRecord(P->ev[2], st));
   // Downward.
   BTK_TRY(run_downward(T, P->ncomp, P->d_T4, w, o, st));
@@ -607,6 +612,7 @@ btk_status btk_plan_last_timing(btk_plan* P, float* ms) {
   BTK_CUDA(cudaEventElapsedTime(&ms[1], P->ev[1], P->ev[2]));
   BTK_CUDA(cudaEventElapsedTime(&ms[2], P->ev[2], P->ev[3]));
   BTK_CUDA(cudaEventElapsedTime(&ms[3], P->ev[0], P->ev[3]));
+  BTK_CUDA(cudaEventElapsedTime(&ms[4], P->ev[4], P->ev[5]));
   return check_status_word(P->d_ticket_status + 1, P->stream);
 }
 

@@ -212,9 +212,10 @@ class Treecode:
         return out
 
     def last_timing(self) -> dict:
-        ms = (ctypes.c_float * 4)()
+        ms = (ctypes.c_float * 5)()
         check(load().btk_plan_last_timing(self._plan, ms))
-        return {"upward": ms[0], "interactions": ms[1], "downward": ms[2], "total": ms[3]}
+        return {"upward": ms[0], "interactions": ms[1], "downward": ms[2], "total": ms[3],
+                "interaction_kernel": ms[4]}
 
     def close(self):
         if self._plan:

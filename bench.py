@@ -1,0 +1,384 @@
+"""Benchmark: 3-D Coulomb treecode solve on one B200 (replicas on N GPUs).
+
+Workload (the headline configuration): N = 1,048,576 points uniform in the
+unit cube (seeded SplitMix64), charges uniform in [-1,1], targets = sources,
+Chebyshev degree n = 8 (729 proxy points per cluster), MAC theta = 0.7, leaf
+size 2000, kernel eps = 1e-4; potential + gradient (field -grad phi).
+
+A step is one full solve (upward pass, PP/PC/CP/CC interactions, downward
+pass) on device-resident inputs; L2 is flushed (256 MB write) before every
+timed step, outside the timed region. ``value`` is interactions (pairwise
+kernel evaluations, at each interaction's degree) per second over the whole
+job; ``e2e`` is the same metric through the C ABI with pinned host buffers,
+the host->device copies of coordinates and charges and the device->host copy
+of the results inside the timed region.
+
+``--impl reference`` times the reference's own CPU implementation (its
+sources compiled with OpenMP against the project's Kokkos-API shim,
+oracle/_ref/libbtkref.so) on this host's cores, on strided samples of the same
+solve.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D N=1M solve ms & interactions/s: learned+FP32 vs plain FP64 at 1e-6 rel L2"
+N_POINTS = 1 << 20  # overridable with --points for small profiling captures
+DEGREE, THETA, LEAF, EPS = 8, 0.7, 2000, 1e-4
+SEED = 1
+# Algorithmic flops per pairwise evaluation (FMA = 2, rsqrt/rcp = 1):
+# 3-D potential 13, potential + Coulomb gradient 24.
+FLOPS_PER_EVAL = {0: 13, 2: 24}
+
+
+def workload_name(kind, precision):
+    what = "potential+gradient" if kind == 2 else "potential"
+    prec = "plain FP64" if precision == 0 else "mixed FP32/FP64"
+    return (f"3D Coulomb {what}, N={N_POINTS} uniform unit cube, charges U[-1,1], n={DEGREE}, theta={THETA}, "
+            f"leaf {LEAF}, eps {EPS}, {prec}")
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = sorted(sm)[len(sm) // 4:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+# ---------------------------------------------------------------- distributed
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- reference arm
+def reference_tree(points, threads):
+    from oracle import RefLib
+    ref = RefLib(threads=threads)
+    return ref.create(3, points, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS)
+
+
+def reference_sample(rt, q, target_seconds):
+    """Strided, timed samples of the reference's own functors (OpenMP build).
+    Potential + gradient = the reference's potential pass plus its gradient-type
+    (velocity) pass over the same pairs. Returns dict(value, est_solve_s, ...)."""
+    # calibrate the stride on a very sparse sample
+    cal = 4096
+    sec, scale, ev = rt.time_sample_3d(0, cal, q)
+    est_full = float(np.sum(sec * scale))
+    stride = max(1, int(np.ceil(2 * est_full / max(target_seconds, 1e-3))))
+    total_s, sampled_s, evals = 0.0, 0.0, 0.0
+    for kind in (0, 1):
+        sec, scale, ev = rt.time_sample_3d(kind, stride, q)
+        total_s += float(np.sum(sec * scale))
+        sampled_s += float(np.sum(sec))
+        evals = float(ev[1])
+    return {"value": evals / total_s, "est_solve_s": total_s, "sampled_s": sampled_s, "stride": stride,
+            "evals": evals}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    from barytreek_b200 import datagen
+    from oracle import RefLib
+    if not RefLib.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libbtkref.so not built (reference tree absent at build)"}
+    pts, q = datagen.uniform_box(SEED, N_POINTS, 3, 0.0, 1.0)
+    cores = cpu_cores()
+    per_step = float(os.environ.get("BTK_REF_STEP_SECONDS", "6"))
+    rt = reference_tree(pts, cores)
+    vals, ests = [], []
+    for i in range(args.warmup + args.steps):
+        r = reference_sample(rt, q, per_step)
+        if i >= args.warmup:
+            vals.append(r["value"])
+            ests.append(r["est_solve_s"])
+    value = statistics.median(vals)
+    sample = (f"every {r['stride']}-th work item of each phase (base_pots, child_to_parent, PP, PC, CP, CC, "
+              f"parent_to_child, leaf_to_point) of the potential pass and of the velocity pass, timed and scaled by "
+              f"work; {r['sampled_s']:.1f} s of CPU work per step")
+    return {"metric": METRIC, "value": value, "unit": "interactions/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(ests), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64)",
+            "impl": "reference",
+            "config": {"workload": workload_name(2, 0), "parallelism": "OpenMP host threads"},
+            "cpu_baseline": {"value": value, "unit": "interactions/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# ---------------------------------------------------------------- native arm
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+def direct_check(tc, q, kind, m=10000):
+    import torch
+    from barytreek_b200 import _lib
+    L = _lib.load()
+    idx = np.sort(np.random.default_rng(12345).choice(tc.nt, m, replace=False))
+    t = [torch.from_numpy(np.ascontiguousarray(c[idx])).cuda() for c in tc.targets]
+    out = torch.empty((tc.ncomp, m), dtype=torch.float64, device="cuda")
+    qd = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    s = tc._s
+    _lib.check(L.btk_direct_sum(3, kind, EPS, m, _lib.ptr(t[0]), _lib.ptr(t[1]), _lib.ptr(t[2]), tc.ns,
+                                _lib.ptr(s[0]), _lib.ptr(s[1]), _lib.ptr(s[2]), _lib.ptr(qd), _lib.ptr(out), None))
+    return idx, out.cpu().numpy()
+
+
+def load_traffic(key):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(path)).get(key)
+    except Exception:
+        return None
+
+
+def run_native(args, world, rank, local):
+    import torch
+    import barytreek_b200 as btk
+    from barytreek_b200 import _lib, datagen
+    L = _lib.load()
+    kind, precision = args.kind, args.precision
+    pts, q = datagen.uniform_box(SEED, N_POINTS, 3, 0.0, 1.0)
+    t0 = time.time()
+    tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind, precision=precision)
+    torch.cuda.synchronize()
+    setup_s = time.time() - t0
+    evals = tc.evals()
+    qd = torch.from_numpy(q).cuda()
+    flush = torch.empty(32 << 20, dtype=torch.float64, device="cuda")  # 256 MB > 126 MB L2
+    for _ in range(args.warmup):
+        tc.solve(qd)
+        tc.last_timing()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = L.btk_launch_count()
+    step_ms, kern_ms, phases = [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            out = tc.solve(qd)
+            t = tc.last_timing()
+            step_ms.append(t["total"])
+            kern_ms.append(t["interaction_kernel"])
+            phases.append(t)
+        torch.cuda.synchronize()
+    launches = (L.btk_launch_count() - launches0) / max(1, args.steps)
+    clocks = clk.summary()
+    total_ms = sum(step_ms)
+    barrier(world)
+    total_ms_max = max_over_ranks(total_ms, world)
+    ms_per_step = total_ms_max / args.steps
+    value = world * evals / (ms_per_step * 1e-3)
+
+    # e2e through the C ABI: pinned host inputs -> device, solve, results -> host.
+    h_in = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (*pts, q)]
+    d_in = [torch.empty_like(a, device="cuda") for a in h_in]
+    h_out = torch.empty((tc.ncomp, tc.nt), dtype=torch.float64).pin_memory()
+    d_out = torch.empty((tc.ncomp, tc.nt), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for h, d in zip(h_in, d_in):
+            d.copy_(h, non_blocking=True)
+        _lib.check(L.btk_plan_execute(tc._plan, _lib.ptr(d_in[0]), _lib.ptr(d_in[1]), _lib.ptr(d_in[2]),
+                                      _lib.ptr(d_in[0]), _lib.ptr(d_in[1]), _lib.ptr(d_in[2]), _lib.ptr(d_in[3]),
+                                      _lib.ptr(d_out), stream.cuda_stream))
+        h_out.copy_(d_out, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = max_over_ranks(sum(e2e_ms), world)
+    e2e_value = world * evals / (e2e_total / args.steps * 1e-3)
+    h2d = sum(h.numel() * h.element_size() for h in h_in)
+    d2h = h_out.numel() * h_out.element_size()
+    ref_out = out.cpu().numpy()
+    assert np.linalg.norm(h_out.numpy() - ref_out) <= 1e-13 * np.linalg.norm(ref_out)
+
+    if rank != 0:
+        return None
+    # accuracy against the FP64 direct sum on a seeded 10k-target subsample
+    idx, ds = direct_check(tc, q, kind)
+    o = out.cpu().numpy()[:, idx]
+    acc = [float(np.linalg.norm(o[c] - ds[c]) / np.linalg.norm(ds[c])) for c in range(tc.ncomp)]
+    acc_all = float(np.linalg.norm(o - ds) / np.linalg.norm(ds))
+    # roofline of the dominant kernel against the live-measured FP64 FMA pipe peak
+    peak = ctypes.c_double()
+    _lib.check(L.btk_measure_pipe_peak(0 if precision == 0 else 1, ctypes.byref(peak), None))
+    kernel_ms = statistics.mean(kern_ms)
+    flops = FLOPS_PER_EVAL[kind] * evals
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    traffic = load_traffic(f"interact_fp64_k{kind}_cfg2")
+    line = {
+        "metric": METRIC, "value": value, "unit": "interactions/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if precision == 0 else "f32+f64",
+        "data": "synthetic: seeded SplitMix64, uniform unit cube, charges U[-1,1]",
+        "config": {"workload": workload_name(kind, precision), "l2": "flushed (256 MB write) before every step",
+                   "parallelism": "replicas" if world > 1 else "single GPU", "interactions_per_solve": evals,
+                   "evals_by_class": {k: v for k, v in tc.stats().items() if k.startswith("evals")}},
+        "roofline": {"bound": "fp64" if precision == 0 else "fp32", "achieved": achieved, "peak": peak.value,
+                     "unit": "TFLOP/s", "frac": achieved / peak.value, "traffic": traffic,
+                     "kernel": "k_interact_fp64 (persistent PP/PC/CP/CC)", "kernel_ms": kernel_ms,
+                     "flops_per_launch": flops,
+                     "peak_source": "measured live: btk_measure_pipe_peak FMA-chain probe on this GPU"},
+        "e2e": {"value": e2e_value, "unit": "interactions/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_total / args.steps},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "accuracy": {"rel_l2_vs_direct_10k": acc_all, "per_component": acc},
+        "phases_ms": {k: statistics.mean(p[k] for p in phases) for k in phases[0]},
+        "setup_s": setup_s,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import RefLib
+        if RefLib.available():
+            r = reference_sample(reference_tree(pts, cpu_cores()), q,
+                                 float(os.environ.get("BTK_CPU_BASELINE_SECONDS", "12")))
+            line["cpu_baseline"] = {
+                "value": r["value"], "unit": "interactions/s", "cores": cpu_cores(), "kind": "reference",
+                "sample": (f"reference functors (OpenMP, Kokkos-API shim build) on every {r['stride']}-th work item "
+                           f"of every phase of the potential and velocity passes, scaled by work; "
+                           f"{r['sampled_s']:.1f} s of CPU work"),
+                "est_solve_s": r["est_solve_s"]}
+        else:
+            line["cpu_baseline"] = None
+    tc.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--kind", type=int, default=2, choices=[0, 2])
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--points", type=int, default=N_POINTS, help="point count (profiling captures only)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    globals()["N_POINTS"] = args.points
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        line = run_reference(args, world, rank)
+    else:
+        world, rank, local = dist_setup(args.gpus)
+        line = run_native(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -291,9 +291,10 @@ btk_status btk_plan_execute(btk_plan* plan, const double* xt, const double* yt, 
                             const double* xs, const double* ys, const double* zs, const double* charges,
                             double* out, btk_stream_t stream);
 
-/* Phase timing of the last btk_plan_execute on this plan (CUDA events; the
- * call synchronises on them). ms[0] upward, [1] interactions, [2] downward,
- * [3] total. */
+/* Phase timing of the last btk_plan_execute on this plan (CUDA events on the
+ * execute stream; the call synchronises on them and reports a device-side
+ * timeout as BTK_ERR_DEVICE_TIMEOUT). ms[0] upward, [1] interaction phase,
+ * [2] downward, [3] total, [4] the interaction kernel alone. */
 btk_status btk_plan_last_timing(btk_plan* plan, float* ms);
 
 /* One call from host buffers: builds the tree and lists with the host tree
@@ -302,6 +303,12 @@ btk_status btk_plan_last_timing(btk_plan* plan, float* ms);
 btk_status btk_solve_host(int dim, int kind, int precision, int degree, int cluster_size, double theta,
                           double eps, int n, const double* x, const double* y, const double* z,
                           const double* charges, double* out, btk_stream_t stream);
+
+/* Sustained fused-multiply-add rate of this GPU's FP64 (which = 0) or FP32
+ * (which = 1) CUDA-core pipe, in TFLOP/s (2 flops per FMA), measured by a
+ * probe kernel with independent FMA chains on every SM. The roofline
+ * denominator for the pairwise interaction kernels. */
+btk_status btk_measure_pipe_peak(int which, double* tflops, btk_stream_t stream);
 
 #ifdef __cplusplus
 }
