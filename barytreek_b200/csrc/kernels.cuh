@@ -41,7 +41,10 @@ struct WorkItem {
   int s_total;         // sources over the entries
   int flags;           // kItemProxyTargets | kItemAtomic
   int pad0, pad1;
+  double cx, cy, cz;   // FP64 centre of the target panel (mixed precision origin)
+  double pad2;
 };
+static_assert(sizeof(WorkItem) == 64, "WorkItem is one 64-byte record");
 constexpr int kItemProxyTargets = 1;  // outputs go to proxy target weights
 constexpr int kItemAtomic = 2;        // another item shares these targets
 

@@ -191,6 +191,206 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed precision: the same pipeline, but every chunk of FP64 sources is
+// rewritten in shared memory as FP32 coordinates relative to the item's FP64
+// target-panel centre (one FP64 subtraction per source per item), and the
+// pairwise arithmetic runs in FP32 with the MUFU approximations. Per target,
+// FP32 partial sums over kFold sources are folded into an FP64 accumulator
+// with a compensated (two-sum) addition, so the final per-target sum carries
+// FP64 precision; the constant factor is applied in FP64 at the end.
+// ---------------------------------------------------------------------------
+constexpr int kFold = 128;
+
+template <int DIM, int KIND>
+__device__ __forceinline__ void eval_fp32(float tx, float ty, float tz, const float4& s, float eps2, float* acc) {
+  const float dx = tx - s.x, dy = ty - s.y;
+  if (DIM == 2) {
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, eps2));
+    acc[0] = fmaf(s.w, __logf(r2), acc[0]);
+    if (KIND == BTK_KIND_FIELD) {
+      const float g = s.w * rcp_fp32(r2);
+      acc[1] = fmaf(dx, g, acc[1]);
+      acc[2] = fmaf(dy, g, acc[2]);
+    }
+  } else {
+    const float dz = tz - s.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+    if (KIND == BTK_KIND_VEL) {
+      const float g = s.w * rcp_fp32(r2);
+      acc[0] = fmaf(dx, g, acc[0]);
+      acc[1] = fmaf(dy, g, acc[1]);
+      acc[2] = fmaf(dz, g, acc[2]);
+    } else {
+      const float ri = rsqrt_fp32(r2);
+      if (KIND == BTK_KIND_POT) {
+        acc[0] = fmaf(s.w, ri, acc[0]);
+      } else {
+        const float wr = s.w * ri;
+        acc[0] += wr;
+        const float g = wr * (ri * ri);
+        acc[1] = fmaf(dx, g, acc[1]);
+        acc[2] = fmaf(dy, g, acc[2]);
+        acc[3] = fmaf(dz, g, acc[3]);
+      }
+    }
+  }
+}
+
+// Knuth's two-sum: s + e == a + b exactly; the error term is kept in `comp`.
+__device__ __forceinline__ void two_sum_add(double& sum, double& comp, double b) {
+  const double s = sum + b;
+  const double bp = s - sum;
+  const double e = (sum - (s - bp)) + (b - bp);
+  sum = s;
+  comp += e;
+}
+
+template <int DIM, int KIND>
+__global__ void __launch_bounds__(kInteractThreads, 6) k_interact_mixed(InteractParams p) {
+  constexpr int NC = KernelTraits<DIM, KIND>::NC;
+  constexpr int TPT = kTargetsPerThread;
+  __shared__ __align__(128) double4 sbuf[kStages][kChunk];
+  __shared__ __align__(16) float4 fbuf[kChunk];
+  __shared__ __align__(8) uint64_t bars[kStages];
+  __shared__ int s_item, s_abort;
+  __shared__ uint32_t s_fail_chunk;
+
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+    s_abort = 0;
+  }
+  __syncthreads();
+  const float eps2 = (float)p.eps2;
+
+  uint32_t g = 0;
+  int pe = 0, poff = 0;
+  uint32_t issued = 0;
+
+  while (true) {
+    if (tid == 0) s_item = atomicAdd(p.ticket, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= p.n_items || s_abort) break;
+    const WorkItem w = p.items[it];
+    const int n_chunks = (w.s_total + kChunk - 1) / kChunk;
+
+    auto issue = [&](int c) {
+      const int stage = (g + c) % kStages;
+      const int need = min(kChunk, w.s_total - c * kChunk);
+      mbar_arrive_expect_tx(&bars[stage], (uint32_t)need * sizeof(double4));
+      int filled = 0;
+      while (filled < need) {
+        const Entry e = p.entries[pe];
+        const int take = min(need - filled, e.s_count - poff);
+        bulk_copy_g2s(&sbuf[stage][filled], p.S4 + e.s_begin + poff, (uint32_t)take * sizeof(double4), &bars[stage]);
+        filled += take;
+        poff += take;
+        if (poff == e.s_count) {
+          ++pe;
+          poff = 0;
+        }
+      }
+      ++issued;
+    };
+    if (tid == 0) {
+      pe = w.e_begin;
+      poff = 0;
+      for (int c = 0; c < min(kStages, n_chunks); ++c) issue(c);
+    }
+
+    float tx[TPT], ty[TPT], tz[TPT];
+    double acc[TPT][NC], comp[TPT][NC];
+#pragma unroll
+    for (int u = 0; u < TPT; ++u) {
+      const int i = min(tid + u * kInteractThreads, w.t_count - 1);
+      const double4 t = p.T4[w.t_begin + i];
+      tx[u] = (float)(t.x - w.cx);
+      ty[u] = (float)(t.y - w.cy);
+      tz[u] = (float)(t.z - w.cz);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[u][c] = comp[u][c] = 0.0;
+    }
+
+    for (int c = 0; c < n_chunks; ++c) {
+      const int stage = (g + c) % kStages;
+      const uint32_t parity = ((g + c) / kStages) & 1u;
+      if (!mbar_wait_bounded(&bars[stage], parity, kWaitLimit)) {
+        s_abort = 1;
+        s_fail_chunk = g + c;
+        atomicCAS(p.status, 0, (int)BTK_ERR_DEVICE_TIMEOUT);
+      }
+      __syncthreads();
+      if (s_abort) break;
+      const int cnt = min(kChunk, w.s_total - c * kChunk);
+      for (int j = tid; j < cnt; j += kInteractThreads) {
+        const double4 s = sbuf[stage][j];
+        fbuf[j] = make_float4((float)(s.x - w.cx), (float)(s.y - w.cy), (float)(s.z - w.cz), (float)s.w);
+      }
+      __syncthreads();
+      // The FP64 stage is free again: refill it while this chunk is evaluated.
+      if (tid == 0 && c + kStages < n_chunks) issue(c + kStages);
+      for (int f0 = 0; f0 < cnt; f0 += kFold) {
+        const int f1 = min(cnt, f0 + kFold);
+        float part[TPT][NC];
+#pragma unroll
+        for (int u = 0; u < TPT; ++u)
+#pragma unroll
+          for (int k = 0; k < NC; ++k) part[u][k] = 0.f;
+#pragma unroll 4
+        for (int j = f0; j < f1; ++j) {
+          const float4 s = fbuf[j];
+#pragma unroll
+          for (int u = 0; u < TPT; ++u) eval_fp32<DIM, KIND>(tx[u], ty[u], tz[u], s, eps2, part[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < TPT; ++u)
+#pragma unroll
+          for (int k = 0; k < NC; ++k) two_sum_add(acc[u][k], comp[u][k], (double)part[u][k]);
+      }
+      __syncthreads();
+    }
+    if (s_abort) break;
+    g += n_chunks;
+
+#pragma unroll
+    for (int u = 0; u < TPT; ++u) {
+      const int i = tid + u * kInteractThreads;
+      if (i < w.t_count) {
+        const int idx = p.T_out[w.t_begin + i];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          double* dst = ((w.flags & kItemProxyTargets) ? p.ptw[c] : p.out[c]) + idx;
+          const double v = (acc[u][c] + comp[u][c]) * p.scale[c];
+          if (w.flags & kItemAtomic)
+            atomicAdd(dst, v);
+          else
+            *dst += v;
+        }
+      }
+    }
+  }
+  if (s_abort && tid == 0) {
+    for (uint32_t k = s_fail_chunk; k < issued; ++k)
+      mbar_wait_bounded(&bars[k % kStages], (k / kStages) & 1u, kWaitLimit);
+  }
+}
+
+template <int DIM, int KIND, bool GUARD>
+cudaError_t launch_mixed(const InteractParams& p, int grid, cudaStream_t s) {
+  k_interact_mixed<DIM, KIND><<<grid, kInteractThreads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <int DIM, int KIND, bool GUARD>
+int occupancy_mixed() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_interact_mixed<DIM, KIND>, kInteractThreads, 0);
+  return n;
+}
+
 template <int DIM, int KIND, bool GUARD>
 cudaError_t launch_fp64(const InteractParams& p, int grid, cudaStream_t s) {
   k_interact_fp64<DIM, KIND, GUARD><<<grid, kInteractThreads, 0, s>>>(p);
@@ -228,11 +428,13 @@ cudaError_t launch_interact(int dim, int kind, int precision, bool guard, const 
   if (p.n_items <= 0) return cudaSuccess;
   count_launch();
   if (precision == BTK_PREC_FP64) BTK_KIND_SWITCH(dim, kind, guard, launch_fp64, p, grid, s);
+  if (precision == BTK_PREC_MIXED) BTK_KIND_SWITCH(dim, kind, false, launch_mixed, p, grid, s);
   return cudaErrorInvalidValue;
 }
 
 int interact_blocks_per_sm(int dim, int kind, int precision, bool guard) {
   if (precision == BTK_PREC_FP64) BTK_KIND_SWITCH(dim, kind, guard, occupancy_fp64);
+  if (precision == BTK_PREC_MIXED) BTK_KIND_SWITCH(dim, kind, false, occupancy_mixed);
   return 0;
 }
 

@@ -279,12 +279,28 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
     const bool proxy = !T.h.is_leaf[tp];
     const int t0 = proxy ? nt + T.cluster_slot[tp] * ipc : T.leaf_begin[tp];
     const int tn = proxy ? ipc : T.h.point_count[tp];
+    // Origin for relative coordinates (mixed precision): the target panel's centre.
+    const PanelGeom& g = T.h.geom[tp];
+    const double c[3] = {0.5 * (g.lo[0] + g.hi[0]), 0.5 * (g.lo[1] + g.hi[1]), 0.5 * (g.lo[2] + g.hi[2])};
+    auto item = [&](int tb, int tc, int kb, int ke, int st, int flags) {
+      WorkItem w{};
+      w.t_begin = tb;
+      w.t_count = tc;
+      w.e_begin = kb;
+      w.e_end = ke;
+      w.s_total = st;
+      w.flags = flags;
+      w.cx = c[0];
+      w.cy = c[1];
+      w.cz = c[2];
+      return w;
+    };
     for (int a = 0; a < tn; a += kTile) {
       const int tc = std::min(kTile, tn - a);
       const int64_t cost = (int64_t)tc * s_total;
       const int nsplit = (int)std::min<int64_t>((cost + max_cost - 1) / max_cost, e1 - e0);
       if (nsplit <= 1) {
-        items.push_back({cost, WorkItem{t0 + a, tc, e0, e1, s_total, proxy ? kItemProxyTargets : 0, 0, 0}});
+        items.push_back({cost, item(t0 + a, tc, e0, e1, s_total, proxy ? kItemProxyTargets : 0)});
         continue;
       }
       // Split the entry range into nsplit pieces of similar source counts.
@@ -293,8 +309,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
       while (k < e1) {
         int kb = k, st = 0;
         while (k < e1 && (st == 0 || st + W.entries[k].s_count <= per)) st += W.entries[k++].s_count;
-        items.push_back({(int64_t)tc * st, WorkItem{t0 + a, tc, kb, k, st,
-                                                     (proxy ? kItemProxyTargets : 0) | kItemAtomic, 0, 0}});
+        items.push_back({(int64_t)tc * st, item(t0 + a, tc, kb, k, st, (proxy ? kItemProxyTargets : 0) | kItemAtomic)});
       }
     }
   }
@@ -432,7 +447,8 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
   BTK_TRY(validate_cfg(&cfg, cfg.dim));
   BTK_CHECK(D->kind >= 0 && D->kind <= 2, BTK_ERR_INVALID_ARGUMENT, "bad kind");
   BTK_CHECK(!(D->kind == BTK_KIND_VEL && cfg.dim != 3), BTK_ERR_UNSUPPORTED, "VEL kernel is 3-D only");
-  BTK_CHECK(D->precision == BTK_PREC_FP64, BTK_ERR_UNSUPPORTED, "precision not available in this build");
+  BTK_CHECK(D->precision == BTK_PREC_FP64 || D->precision == BTK_PREC_MIXED, BTK_ERR_UNSUPPORTED,
+            "precision must be BTK_PREC_FP64 or BTK_PREC_MIXED");
   BTK_CHECK(D->tree_target && D->panels_target && D->panel_points_inside_target && D->point_leaf_panel_source,
             BTK_ERR_INVALID_ARGUMENT, "plan: missing tree arrays");
   P->dim = cfg.dim;
