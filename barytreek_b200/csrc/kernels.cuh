@@ -40,7 +40,8 @@ struct WorkItem {
   int e_begin, e_end;  // entry range
   int s_total;         // sources over the entries
   int flags;           // kItemProxyTargets | kItemAtomic
-  int pad0, pad1;
+  int near_total;      // the first near_total sources are PP (near-field) points
+  int pad1;
   double cx, cy, cz;   // FP64 centre of the target panel (mixed precision origin)
   double pad2;
 };

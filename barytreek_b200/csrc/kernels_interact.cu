@@ -202,9 +202,15 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
 // ---------------------------------------------------------------------------
 constexpr int kFold = 128;
 
-template <int DIM, int KIND>
-__device__ __forceinline__ void eval_fp32(float tx, float ty, float tz, const float4& s, float eps2, float* acc) {
-  const float dx = tx - s.x, dy = ty - s.y;
+// NEAR: coordinates carry an FP32 low part (x = hi + lo, both relative to the
+// item's centre), and the difference is formed as (t_hi - s_hi) + (t_lo - s_lo)
+// so near-field pairs (PP) keep their separation to ~1e-14 relative to the
+// centre distance, not FP32's 6e-8.
+template <int DIM, int KIND, bool NEAR>
+__device__ __forceinline__ void eval_fp32(float tx, float ty, float tz, float lx, float ly, float lz, const float4& s,
+                                          const float4& sl, float eps2, float* acc) {
+  const float dx = NEAR ? (tx - s.x) + (lx - sl.x) : tx - s.x;
+  const float dy = NEAR ? (ty - s.y) + (ly - sl.y) : ty - s.y;
   if (DIM == 2) {
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, eps2));
     acc[0] = fmaf(s.w, __logf(r2), acc[0]);
@@ -214,7 +220,7 @@ __device__ __forceinline__ void eval_fp32(float tx, float ty, float tz, const fl
       acc[2] = fmaf(dy, g, acc[2]);
     }
   } else {
-    const float dz = tz - s.z;
+    const float dz = NEAR ? (tz - s.z) + (lz - sl.z) : tz - s.z;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
     if (KIND == BTK_KIND_VEL) {
       const float g = s.w * rcp_fp32(r2);
@@ -237,6 +243,13 @@ __device__ __forceinline__ void eval_fp32(float tx, float ty, float tz, const fl
   }
 }
 
+// x - c split into FP32 hi + lo (hi = x - c rounded, lo = the FP32-rounded rest).
+__device__ __forceinline__ void split_rel(double x, double c, float& hi, float& lo) {
+  const double r = x - c;
+  hi = (float)r;
+  lo = (float)(r - (double)hi);
+}
+
 // Knuth's two-sum: s + e == a + b exactly; the error term is kept in `comp`.
 __device__ __forceinline__ void two_sum_add(double& sum, double& comp, double b) {
   const double s = sum + b;
@@ -251,7 +264,7 @@ __global__ void __launch_bounds__(kInteractThreads, 6) k_interact_mixed(Interact
   constexpr int NC = KernelTraits<DIM, KIND>::NC;
   constexpr int TPT = kTargetsPerThread;
   __shared__ __align__(128) double4 sbuf[kStages][kChunk];
-  __shared__ __align__(16) float4 fbuf[kChunk];
+  __shared__ __align__(16) float4 fbuf[kChunk], fbuf_lo[kChunk];
   __shared__ __align__(8) uint64_t bars[kStages];
   __shared__ int s_item, s_abort;
   __shared__ uint32_t s_fail_chunk;
@@ -301,15 +314,15 @@ __global__ void __launch_bounds__(kInteractThreads, 6) k_interact_mixed(Interact
       for (int c = 0; c < min(kStages, n_chunks); ++c) issue(c);
     }
 
-    float tx[TPT], ty[TPT], tz[TPT];
+    float tx[TPT], ty[TPT], tz[TPT], lx[TPT], ly[TPT], lz[TPT];
     double acc[TPT][NC], comp[TPT][NC];
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
       const int i = min(tid + u * kInteractThreads, w.t_count - 1);
       const double4 t = p.T4[w.t_begin + i];
-      tx[u] = (float)(t.x - w.cx);
-      ty[u] = (float)(t.y - w.cy);
-      tz[u] = (float)(t.z - w.cz);
+      split_rel(t.x, w.cx, tx[u], lx[u]);
+      split_rel(t.y, w.cy, ty[u], ly[u]);
+      split_rel(t.z, w.cz, tz[u], lz[u]);
 #pragma unroll
       for (int c = 0; c < NC; ++c) acc[u][c] = comp[u][c] = 0.0;
     }
@@ -325,9 +338,17 @@ __global__ void __launch_bounds__(kInteractThreads, 6) k_interact_mixed(Interact
       __syncthreads();
       if (s_abort) break;
       const int cnt = min(kChunk, w.s_total - c * kChunk);
+      const int near_end = min(cnt, max(0, w.near_total - c * kChunk));  // near sources of this chunk
       for (int j = tid; j < cnt; j += kInteractThreads) {
         const double4 s = sbuf[stage][j];
-        fbuf[j] = make_float4((float)(s.x - w.cx), (float)(s.y - w.cy), (float)(s.z - w.cz), (float)s.w);
+        float4 h, l;
+        split_rel(s.x, w.cx, h.x, l.x);
+        split_rel(s.y, w.cy, h.y, l.y);
+        split_rel(s.z, w.cz, h.z, l.z);
+        h.w = (float)s.w;
+        l.w = 0.f;
+        fbuf[j] = h;
+        fbuf_lo[j] = l;
       }
       __syncthreads();
       // The FP64 stage is free again: refill it while this chunk is evaluated.
@@ -339,11 +360,20 @@ __global__ void __launch_bounds__(kInteractThreads, 6) k_interact_mixed(Interact
         for (int u = 0; u < TPT; ++u)
 #pragma unroll
           for (int k = 0; k < NC; ++k) part[u][k] = 0.f;
+        const int fn = min(f1, max(f0, near_end));
+#pragma unroll 2
+        for (int j = f0; j < fn; ++j) {
+          const float4 s = fbuf[j], sl = fbuf_lo[j];
+#pragma unroll
+          for (int u = 0; u < TPT; ++u)
+            eval_fp32<DIM, KIND, true>(tx[u], ty[u], tz[u], lx[u], ly[u], lz[u], s, sl, eps2, part[u]);
+        }
 #pragma unroll 4
-        for (int j = f0; j < f1; ++j) {
+        for (int j = fn; j < f1; ++j) {
           const float4 s = fbuf[j];
 #pragma unroll
-          for (int u = 0; u < TPT; ++u) eval_fp32<DIM, KIND>(tx[u], ty[u], tz[u], s, eps2, part[u]);
+          for (int u = 0; u < TPT; ++u)
+            eval_fp32<DIM, KIND, false>(tx[u], ty[u], tz[u], lx[u], ly[u], lz[u], s, s, eps2, part[u]);
         }
 #pragma unroll
         for (int u = 0; u < TPT; ++u)

@@ -243,10 +243,12 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
   for (int i = 0; i < Pt; ++i) head[i + 1] += head[i];
   std::vector<Entry> grouped(head[Pt]);
   std::vector<int> cur(head.begin(), head.end() - 1);
+  std::vector<int> n_near(Pt, 0);  // PP entries lead each target's group
   for (int t = 0; t < 4; ++t)
     for (int i = 0; i < counts[t]; ++i) {
       const btk_interact_pair& pr = lists[t][i];
       const int sp = pr.source_panel, tp = pr.target_panel;
+      if (t == 0) n_near[tp]++;
       Entry e;
       if (t & 1) {  // cluster source: its proxies
         e.s_begin = ns + S.cluster_slot[sp] * ipc;
@@ -268,13 +270,21 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
     const int eb = head[tp], ee = head[tp + 1];
     if (eb == ee) continue;
     const int e0 = (int)W.entries.size();
-    int s_total = 0;
-    for (int k = eb; k < ee; ++k)
+    int s_total = 0, e_near = e0;
+    for (int k = eb; k < ee; ++k) {
       if (grouped[k].s_count > 0) {
         W.entries.push_back(grouped[k]);
         s_total += grouped[k].s_count;
       }
+      if (k - eb < n_near[tp]) e_near = (int)W.entries.size();
+    }
     const int e1 = (int)W.entries.size();
+    // Sources of entries [kb, ke) that are near-field (PP) points.
+    auto near_of = [&](int kb, int ke) {
+      int n = 0;
+      for (int k = kb; k < std::min(ke, e_near); ++k) n += W.entries[k].s_count;
+      return n;
+    };
     if (s_total == 0) continue;
     const bool proxy = !T.h.is_leaf[tp];
     const int t0 = proxy ? nt + T.cluster_slot[tp] * ipc : T.leaf_begin[tp];
@@ -290,6 +300,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
       w.e_end = ke;
       w.s_total = st;
       w.flags = flags;
+      w.near_total = near_of(kb, ke);
       w.cx = c[0];
       w.cy = c[1];
       w.cz = c[2];

@@ -82,6 +82,29 @@ class Oracle:
                                        vp, ci, vp, ci, vp, ci, vp, ci, vp, ci, vp, vp]
         L.bto_downward.argtypes = [ci, ci, ci, ci, ci, vp, vp, vp, ci, vp, vp, ci, vp, vp, vp]
         L.bto_direct.argtypes = [ci, ci, cd, ci, vp, vp, vp, ci, vp, vp, vp, vp, vp]
+        L.bto_solve_degrees.argtypes = [ci, ci, ci, cd, ci, ci, vp, vp, vp, ci, vp, vp, vp, vp, vp, ci, vp, vp, ci,
+                                        vp, vp, ci, vp, ci, vp, vp, ci, vp, vp, ci, vp, vp]
+
+    def solve_degrees(self, tree, kind, q, deg_pc=None, deg_cp=None, deg_cc=None):
+        """Treecode with one degree per far-field pair (bto_solve_degrees)."""
+        dim, eps, thresh = tree["dim"], tree["eps"], tree["thresh"]
+        tg = [_f64(a) for a in tree["targets"]] + [None] * (3 - dim)
+        sc = [_f64(a) for a in tree["sources"]] + [None] * (3 - dim)
+        q = _f64(q)
+        nt, ns = len(tg[0]), len(sc[0])
+        out = np.zeros((ncomp(dim, kind), nt))
+        L = {k: np.ascontiguousarray(tree[k], PAIR_DTYPE) for k in ("pp", "pc", "cp", "cc")}
+        dg = [None if d is None else np.ascontiguousarray(d, np.int32) for d in (deg_pc, deg_cp, deg_cc)]
+        rc = self.lib.bto_solve_degrees(
+            dim, kind, tree["degree"], eps, thresh, nt, _p(tg[0]), _p(tg[1]), _p(tg[2]), ns, _p(sc[0]), _p(sc[1]),
+            _p(sc[2]), _p(q), _p(tree["panels_t"]), len(tree["panels_t"]),
+            _p(np.ascontiguousarray(tree["inside_t"], np.int32)), _p(tree["panels_s"]), len(tree["panels_s"]),
+            _p(np.ascontiguousarray(tree["inside_s"], np.int32)), _p(L["pp"]), len(L["pp"]), _p(L["pc"]),
+            len(L["pc"]), _p(dg[0]), _p(L["cp"]), len(L["cp"]), _p(dg[1]), _p(L["cc"]), len(L["cc"]), _p(dg[2]),
+            _p(out))
+        if rc:
+            raise RuntimeError("bto_solve_degrees failed")
+        return out
 
     def interp_basis(self, x, lo, hi, n):
         out = np.zeros(n + 1)

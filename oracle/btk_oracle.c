@@ -333,3 +333,133 @@ int bto_direct(int dim, int kind, double eps, int nt, const double* tx, const do
   }
   return 0;
 }
+
+/* ---- per-pair degrees (learned-degree extension) ------------------------- */
+
+/* Appends the points under panel p (all leaves of its subtree) to buf. */
+static void subtree_points(int dim, const void* panels, const int* inside, int thresh, int p, int* buf, int* n) {
+  pnl P = get_panel(dim, panels, p);
+  if (P.leaf) {
+    for (int j = 0; j < P.count; ++j) buf[(*n)++] = inside[(size_t)p * thresh + j];
+    return;
+  }
+  for (int c = 0; c < P.nchild; ++c) subtree_points(dim, panels, inside, thresh, P.child[c], buf, n);
+}
+
+/* Modified charges at degree d of the given points on panel S's box. */
+static void charges_at_degree(int dim, int d, const pnl* S, const int* idx, int n, const double* sx, const double* sy,
+                              const double* sz, const double* q, double* Q) {
+  int ipc = ipow(d + 1, dim);
+  memset(Q, 0, sizeof(double) * ipc);
+  for (int i = 0; i < n; ++i) {
+    int s = idx[i];
+    double pt[3] = {sx[s], sy[s], dim == 3 ? sz[s] : 0.0};
+    double b[3][MAXD];
+    for (int a = 0; a < dim; ++a) bto_interp_basis(b[a], pt[a], S->lo[a], S->hi[a], d);
+    for (int k = 0; k < ipc; ++k) Q[k] += basis_prod(dim, d, b, k) * q[s];
+  }
+}
+
+int bto_solve_degrees(int dim, int kind, int degree, double eps, int thresh, int n_tgt, const double* tx,
+                      const double* ty, const double* tz, int n_src, const double* sx, const double* sy,
+                      const double* sz, const double* q, const void* panels_t, int panel_count_t,
+                      const int* inside_t, const void* panels_s, int panel_count_s, const int* inside_s,
+                      const bto_pair* pp, int n_pp, const bto_pair* pc, int n_pc, const int* deg_pc,
+                      const bto_pair* cp, int n_cp, const int* deg_cp, const bto_pair* cc, int n_cc,
+                      const int* deg_cc, double* out) {
+  (void)panel_count_t;
+  (void)panel_count_s;
+  const int nc = bto_ncomp(dim, kind);
+  const double eps2 = eps * eps;
+  const int maxipc = ipow(MAXD, dim);
+  int* tbuf = (int*)malloc(sizeof(int) * (n_tgt > 0 ? n_tgt : 1));
+  int* sbuf = (int*)malloc(sizeof(int) * (n_src > 0 ? n_src : 1));
+  double* Q = (double*)malloc(sizeof(double) * maxipc);
+  double* Phi = (double*)malloc(sizeof(double) * maxipc * 4);
+  if (!tbuf || !sbuf || !Q || !Phi) return 1;
+  memset(out, 0, sizeof(double) * (size_t)nc * n_tgt);
+  double acc[4];
+  /* PP exactly as the reference */
+  for (int e = 0; e < n_pp; ++e) {
+    pnl T = get_panel(dim, panels_t, pp[e].target_panel), S = get_panel(dim, panels_s, pp[e].source_panel);
+    for (int j = 0; j < T.count; ++j) {
+      int it = inside_t[(size_t)pp[e].target_panel * thresh + j];
+      double t[3] = {tx[it], ty[it], dim == 3 ? tz[it] : 0.0};
+      memset(acc, 0, sizeof(acc));
+      for (int k = 0; k < S.count; ++k) {
+        int is = inside_s[(size_t)pp[e].source_panel * thresh + k];
+        double s[3] = {sx[is], sy[is], dim == 3 ? sz[is] : 0.0};
+        eval(dim, kind, eps2, t, s, q[is], acc);
+      }
+      for (int c = 0; c < nc; ++c) out[(size_t)c * n_tgt + it] += acc[c];
+    }
+  }
+  const bto_pair* lists[3] = {pc, cp, cc};
+  const int counts[3] = {n_pc, n_cp, n_cc};
+  const int* degs[3] = {deg_pc, deg_cp, deg_cc};
+  for (int L = 0; L < 3; ++L) {
+    for (int e = 0; e < counts[L]; ++e) {
+      const bto_pair pr = lists[L][e];
+      const int d = degs[L] ? degs[L][e] : degree;
+      const int ipc = ipow(d + 1, dim);
+      pnl T = get_panel(dim, panels_t, pr.target_panel), S = get_panel(dim, panels_s, pr.source_panel);
+      double tn[3][MAXD], sn[3][MAXD];
+      panel_nodes(dim, d, &T, tn);
+      panel_nodes(dim, d, &S, sn);
+      int ns_ = 0, nt_ = 0;
+      subtree_points(dim, panels_s, inside_s, thresh, pr.source_panel, sbuf, &ns_);
+      subtree_points(dim, panels_t, inside_t, thresh, pr.target_panel, tbuf, &nt_);
+      if (L == 0) { /* PC */
+        charges_at_degree(dim, d, &S, sbuf, ns_, sx, sy, sz, q, Q);
+        for (int j = 0; j < nt_; ++j) {
+          int it = tbuf[j];
+          double t[3] = {tx[it], ty[it], dim == 3 ? tz[it] : 0.0};
+          memset(acc, 0, sizeof(acc));
+          for (int k = 0; k < ipc; ++k) {
+            double s[3];
+            proxy_point(dim, d, sn, k, s);
+            eval(dim, kind, eps2, t, s, Q[k], acc);
+          }
+          for (int c = 0; c < nc; ++c) out[(size_t)c * n_tgt + it] += acc[c];
+        }
+        continue;
+      }
+      if (L == 2) charges_at_degree(dim, d, &S, sbuf, ns_, sx, sy, sz, q, Q);
+      for (int jj = 0; jj < ipc; ++jj) {
+        double t[3];
+        proxy_point(dim, d, tn, jj, t);
+        memset(acc, 0, sizeof(acc));
+        if (L == 1) { /* CP: S is a leaf, its own points */
+          for (int k = 0; k < ns_; ++k) {
+            int is = sbuf[k];
+            double s[3] = {sx[is], sy[is], dim == 3 ? sz[is] : 0.0};
+            eval(dim, kind, eps2, t, s, q[is], acc);
+          }
+        } else { /* CC */
+          for (int k = 0; k < ipc; ++k) {
+            double s[3];
+            proxy_point(dim, d, sn, k, s);
+            eval(dim, kind, eps2, t, s, Q[k], acc);
+          }
+        }
+        for (int c = 0; c < nc; ++c) Phi[(size_t)c * ipc + jj] = acc[c];
+      }
+      for (int j = 0; j < nt_; ++j) {
+        int it = tbuf[j];
+        double t[3] = {tx[it], ty[it], dim == 3 ? tz[it] : 0.0};
+        double b[3][MAXD];
+        for (int a = 0; a < dim; ++a) bto_interp_basis(b[a], t[a], T.lo[a], T.hi[a], d);
+        for (int c = 0; c < nc; ++c) {
+          double s = 0.0;
+          for (int k = 0; k < ipc; ++k) s += Phi[(size_t)c * ipc + k] * basis_prod(dim, d, b, k);
+          out[(size_t)c * n_tgt + it] += s;
+        }
+      }
+    }
+  }
+  free(tbuf);
+  free(sbuf);
+  free(Q);
+  free(Phi);
+  return 0;
+}

@@ -84,6 +84,26 @@ int bto_downward(int dim, int ncomp, int degree, int thresh, int n_tgt, const do
                  const double* tz, int panel_count, const void* panels, const int* level_start, int levels,
                  const int* inside, double* ptw, double* out);
 
+/* Treecode with a degree per far-field pair (the learned-degree extension; no
+ * reference counterpart). PP as the reference; every PC/CP/CC pair (T, S) at
+ * its own degree d is evaluated straight at the target points:
+ *   Q^d_S  = modified charges of all points under S at degree d
+ *            (base_pots at degree d on S's box),
+ *   PC     : phi(t) += sum_k G(t, x^d_k(S)) Q^d_S[k]      for t in leaf T,
+ *   CP, CC : Phi^d_T[j] = sum over S's points (CP) or proxies (CC) of
+ *            G(x^d_j(T), s) w_s, then phi(t) += sum_j Phi^d_T[j] L^d_j(t) for
+ *            every point t under T.
+ * This equals the tree's anterpolate/transfer/promote/downward chain exactly
+ * in exact arithmetic (polynomial reproduction). out[ncomp][n_tgt] is
+ * overwritten. deg_* may be NULL (then `degree` is used for that class). */
+int bto_solve_degrees(int dim, int kind, int degree, double eps, int thresh, int n_tgt, const double* tx,
+                      const double* ty, const double* tz, int n_src, const double* sx, const double* sy,
+                      const double* sz, const double* q, const void* panels_t, int panel_count_t,
+                      const int* inside_t, const void* panels_s, int panel_count_s, const int* inside_s,
+                      const bto_pair* pp, int n_pp, const bto_pair* pc, int n_pc, const int* deg_pc,
+                      const bto_pair* cp, int n_cp, const int* deg_cp, const bto_pair* cc, int n_cc,
+                      const int* deg_cc, double* out);
+
 /* O(nt*ns) direct sum including i==j (src/direct_sum_impl.hpp:9-94).
  * out[ncomp][nt] is overwritten. */
 int bto_direct(int dim, int kind, double eps, int nt, const double* tx, const double* ty, const double* tz,
