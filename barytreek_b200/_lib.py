@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "libbarytreek_b200.so")
 OK, ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_UNSUPPORTED, ERR_OUT_OF_MEMORY, ERR_DEVICE_TIMEOUT, ERR_IO, ERR_INTERNAL = range(8)
 KIND_POT, KIND_VEL, KIND_FIELD = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+DEGREE_FIXED, DEGREE_PER_PAIR = 0, 1
 
 # Reference struct layouts (src/structs.hpp), as numpy dtypes for host arrays.
 PANEL2_DTYPE = np.dtype({
@@ -57,7 +58,8 @@ class PlanDesc(ctypes.Structure):
                 ("panel_points_inside_target", ctypes.c_void_p), ("panel_points_inside_source", ctypes.c_void_p),
                 ("point_leaf_panel_source", ctypes.c_void_p), ("pp_list", ctypes.c_void_p),
                 ("pc_list", ctypes.c_void_p), ("cp_list", ctypes.c_void_p), ("cc_list", ctypes.c_void_p),
-                ("kind", ctypes.c_int), ("precision", ctypes.c_int)]
+                ("kind", ctypes.c_int), ("precision", ctypes.c_int), ("degree_mode", ctypes.c_int),
+                ("degree_min", ctypes.c_int)]
 
 
 class PlanStats(ctypes.Structure):
@@ -105,6 +107,7 @@ SIGNATURES = {
     "btk_plan_last_timing": [_vp, _vp],
     "btk_solve_host": [_ci, _ci, _ci, _ci, _ci, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_measure_pipe_peak": [_ci, _vp, _vp],
+    "btk_plan_set_degrees": [_vp, _vp, _vp, _vp],
 }
 _RESTYPES = {"btk_last_error": ctypes.c_char_p, "btk_version": ctypes.c_char_p, "btk_launch_count": ctypes.c_uint64,
              "btk_free": None}

@@ -105,4 +105,23 @@ int interact_blocks_per_sm(int dim, int kind, int precision, bool guard);
 cudaError_t launch_direct(int dim, int kind, double eps, int nt, const double* xt, const double* yt,
                           const double* zt, int ns, const double4* src, double* out, cudaStream_t s);
 
+// ---- per-pair degrees (kernels_degree.cu) -------------------------------------
+cudaError_t launch_src_slots(int dim, int n, int n_slots, const int* slot_cluster_panel, const int* slot_degree,
+                             const long long* slot_offset, const DevPanel* panels, const double* psw,
+                             const double* amat, const int* amat_off, const double* ucos_all, const int* ucos_off,
+                             double4* S4, cudaStream_t s);
+cudaError_t launch_tgt_slots(int dim, int n_slots, const int* slot_cluster_panel, const int* slot_degree,
+                             const long long* slot_offset, const DevPanel* panels, const double* ucos_all,
+                             const int* ucos_off, double4* T4, int* T_out, long long t4_base, cudaStream_t s);
+cudaError_t launch_promote(int dim, int n, int ncomp, int n_clusters, const int* cluster_panel,
+                           const int* cluster_slot_begin, const int* slot_degree, const long long* slot_offset,
+                           const double* amat, const int* amat_off, Ptr4 ptwm, Ptr4 ptw, cudaStream_t s);
+cudaError_t launch_resolve(int dim, int n_pc, const int* pc_entry, const int* pc_src_cluster, const int* deg_pc,
+                           int n_far, int tiles_max, const int* far_type, const int* far_tgt_cluster,
+                           const int* far_src, const int* deg_far, const long long* src_slot_offset,
+                           const int* cluster_slot_begin_s, const long long* tgt_slot_offset,
+                           const int* cluster_slot_begin_t, int slot_d_lo, long long t4_base, long long s4_base,
+                           const double* tgt_centre, int n_point_items, WorkItem* items, Entry* entries,
+                           int far_item0, int far_entry0, cudaStream_t s);
+
 }  // namespace btk

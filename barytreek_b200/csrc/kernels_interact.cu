@@ -98,11 +98,13 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
   uint32_t issued = 0;  // global chunk index of the next issue (thread 0)
 
   while (true) {
+    __syncthreads();  // every thread has read the previous ticket
     if (tid == 0) s_item = atomicAdd(p.ticket, 1);
     __syncthreads();
     const int it = s_item;
     if (it >= p.n_items || s_abort) break;
     const WorkItem w = p.items[it];
+    if (w.t_count <= 0 || w.s_total <= 0) continue;  // unused tile of a per-pair-degree item block
     const int n_chunks = (w.s_total + kChunk - 1) / kChunk;
 
     auto issue = [&](int c) {  // thread 0 only: fill chunk c of this item
@@ -283,11 +285,13 @@ __global__ void __launch_bounds__(kInteractThreads, 6) k_interact_mixed(Interact
   uint32_t issued = 0;
 
   while (true) {
+    __syncthreads();  // every thread has read the previous ticket
     if (tid == 0) s_item = atomicAdd(p.ticket, 1);
     __syncthreads();
     const int it = s_item;
     if (it >= p.n_items || s_abort) break;
     const WorkItem w = p.items[it];
+    if (w.t_count <= 0 || w.s_total <= 0) continue;  // unused tile of a per-pair-degree item block
     const int n_chunks = (w.s_total + kChunk - 1) / kChunk;
 
     auto issue = [&](int c) {

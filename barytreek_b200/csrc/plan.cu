@@ -220,8 +220,12 @@ struct WorkLists {
   int64_t evals[4] = {0, 0, 0, 0};
 };
 
-btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lists[4], const int counts[4],
-                      int grid_slots, WorkLists& W) {
+// pc_begin (optional): S4 start of each PC pair's source proxies (default: the
+// cluster's single-degree slot). pc_entry (optional, out): final entry index of
+// each PC pair, for re-pointing when per-pair degrees change.
+btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* const lists[4], const int counts[4],
+                      int grid_slots, WorkLists& W, const std::vector<long long>* pc_begin = nullptr,
+                      std::vector<int>* pc_entry = nullptr) {
   const int ipc = S.ipc;
   const int nt = T.n_points, ns = S.n_points;
   const int Pt = T.h.panel_count, Ps = S.h.panel_count;
@@ -244,6 +248,8 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
   std::vector<Entry> grouped(head[Pt]);
   std::vector<int> cur(head.begin(), head.end() - 1);
   std::vector<int> n_near(Pt, 0);  // PP entries lead each target's group
+  std::vector<int> final_index(head[Pt], -1);
+  if (pc_entry) pc_entry->assign(counts[1], -1);
   for (int t = 0; t < 4; ++t)
     for (int i = 0; i < counts[t]; ++i) {
       const btk_interact_pair& pr = lists[t][i];
@@ -251,7 +257,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
       if (t == 0) n_near[tp]++;
       Entry e;
       if (t & 1) {  // cluster source: its proxies
-        e.s_begin = ns + S.cluster_slot[sp] * ipc;
+        e.s_begin = (t == 1 && pc_begin) ? (int)(*pc_begin)[i] : ns + S.cluster_slot[sp] * ipc;
         e.s_count = ipc;
       } else {
         e.s_begin = S.leaf_begin[sp];
@@ -259,6 +265,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
       }
       const int64_t nt_pts = (t >= 2) ? ipc : T.h.point_count[tp];
       W.evals[t] += nt_pts * (int64_t)e.s_count;
+      if (t == 1 && pc_entry) (*pc_entry)[i] = cur[tp];  // grouped position; remapped below
       grouped[cur[tp]++] = e;
     }
   // Tiles and items.
@@ -273,6 +280,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
     int s_total = 0, e_near = e0;
     for (int k = eb; k < ee; ++k) {
       if (grouped[k].s_count > 0) {
+        final_index[k] = (int)W.entries.size();
         W.entries.push_back(grouped[k]);
         s_total += grouped[k].s_count;
       }
@@ -324,6 +332,8 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* lis
       }
     }
   }
+  if (pc_entry)
+    for (int& k : *pc_entry) k = k >= 0 ? final_index[k] : -1;
   std::stable_sort(items.begin(), items.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
   W.items.resize(items.size());
   for (size_t i = 0; i < items.size(); ++i) W.items[i] = items[i].second;
@@ -446,11 +456,219 @@ struct btk_plan {
   int* d_ticket_status = nullptr;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool timed = false;
+
+  // ---- per-pair degrees (degree_mode == BTK_DEGREE_PER_PAIR) ----
+  int degree_mode = BTK_DEGREE_FIXED, degree_min = 0;
+  int n_pc = 0, n_cp = 0, n_far = 0, tiles_max = 0, n_static_items = 0, n_static_entries = 0;
+  int n_src_slots = 0, n_tgt_slots = 0;
+  long long total_src_slots = 0, total_tgt_slots = 0;
+  int *d_s_slot_panel = nullptr, *d_s_slot_deg = nullptr, *d_s_cluster_slot_begin = nullptr;
+  int *d_t_slot_deg = nullptr, *d_t_cluster_slot_begin = nullptr, *d_t_cluster_panel = nullptr;
+  long long *d_s_slot_off = nullptr, *d_t_slot_off = nullptr;
+  double* d_amat = nullptr;
+  int* d_amat_off = nullptr;
+  double* d_ucos = nullptr;
+  int* d_ucos_off = nullptr;
+  int *d_pc_entry = nullptr, *d_pc_src_cluster = nullptr;
+  int *d_far_type = nullptr, *d_far_tgt = nullptr, *d_far_src = nullptr;
+  double* d_tgt_centre = nullptr;
+  int *d_deg_pc = nullptr, *d_deg_far = nullptr;  // the degrees in force
+  double* d_ptwm = nullptr;                       // ncomp x total_tgt_slots
+  // host copies for work accounting
+  std::vector<int> h_pc_tcount, h_cp_scount, h_deg_pc, h_deg_far;
 };
 
 using namespace btk;
 
 namespace {
+
+// Barycentric basis of degree d on [-1, 1] (nodes cos(pi*a/d)) at x, with the
+// reference's near-node rule (src/bli_impl.hpp:9-63).
+void bary_row_unit(double x, int d, double* out) {
+  const double pi = 3.141592653589793238462643383279502884;
+  std::vector<double> node(d + 1), w(d + 1);
+  for (int a = 0; a <= d; ++a) {
+    node[a] = std::cos(pi * a / d);
+    w[a] = (a % 2 ? -1.0 : 1.0) * ((a == 0 || a == d) ? 0.5 : 1.0);
+  }
+  for (int a = 0; a <= d; ++a)
+    if (std::fabs(x - node[a]) < 2.220446049250313e-16) {
+      for (int b = 0; b <= d; ++b) out[b] = b == a ? 1.0 : 0.0;
+      return;
+    }
+  double den = 0.0;
+  for (int a = 0; a <= d; ++a) {
+    out[a] = w[a] / (x - node[a]);
+    den += out[a];
+  }
+  for (int a = 0; a <= d; ++a) out[a] /= den;
+}
+
+// Far-field evaluation counts at the per-pair degrees in force.
+void recount_far_evals(btk_plan* P) {
+  auto sz = [&](int d) { return (int64_t)ipow(d + 1, P->dim); };
+  P->evals[1] = P->evals[2] = P->evals[3] = 0;
+  for (int i = 0; i < P->n_pc; ++i) P->evals[1] += P->h_pc_tcount[i] * sz(P->h_deg_pc[i]);
+  for (int i = 0; i < P->n_cp; ++i) P->evals[2] += sz(P->h_deg_far[i]) * P->h_cp_scount[i];
+  for (int i = P->n_cp; i < P->n_far; ++i) P->evals[3] += sz(P->h_deg_far[i]) * sz(P->h_deg_far[i]);
+}
+
+btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists[4], const int counts[4], int slots,
+                               cudaStream_t st) {
+  Arena& A = *P->arena;
+  Side& T = P->tgt;
+  Side& S = *P->src;
+  const int dim = P->dim, n = P->degree, dlo = P->degree_min;
+  BTK_CHECK(dlo >= 1 && dlo <= n, BTK_ERR_INVALID_ARGUMENT, "degree_min must be in [1, interp_degree]");
+  const int nd = n - dlo + 1;
+  const int ncs = (int)S.clusters.size(), nct = (int)T.clusters.size();
+  auto sz = [&](int d) { return (long long)ipow(d + 1, dim); };
+  // Slot tables: cluster-major, degrees dlo..n.
+  auto make_slots = [&](const Side& X, std::vector<int>& panel, std::vector<int>& deg, std::vector<long long>& off,
+                        std::vector<int>& begin) {
+    const int nc = (int)X.clusters.size();
+    long long o = 0;
+    begin.resize(nc + 1);
+    for (int c = 0; c < nc; ++c) {
+      begin[c] = c * nd;
+      for (int d = dlo; d <= n; ++d) {
+        panel.push_back(X.clusters[c]);
+        deg.push_back(d);
+        off.push_back(o);
+        o += sz(d);
+      }
+    }
+    begin[nc] = nc * nd;
+    return o;
+  };
+  std::vector<int> s_panel, s_deg, s_begin, t_panel, t_deg, t_begin;
+  std::vector<long long> s_off, t_off;
+  P->total_src_slots = make_slots(S, s_panel, s_deg, s_off, s_begin);
+  P->total_tgt_slots = make_slots(T, t_panel, t_deg, t_off, t_begin);
+  P->n_src_slots = (int)s_panel.size();
+  P->n_tgt_slots = (int)t_panel.size();
+  BTK_CHECK(S.n_points + P->total_src_slots < (1LL << 31) && T.n_points + P->total_tgt_slots < (1LL << 31),
+            BTK_ERR_UNSUPPORTED, "per-pair degree slots exceed 2^31 entries");
+  // Degree transfer matrices A_d[a][i] = L^d_a(x^n_i) (d < n) and unit nodes.
+  std::vector<double> amat, ucos;
+  std::vector<int> amat_off(kMaxNodes, 0), ucos_off(kMaxNodes, 0);
+  const double pi = 3.141592653589793238462643383279502884;
+  for (int d = dlo; d <= n; ++d) {
+    amat_off[d] = (int)amat.size();
+    if (d == n) continue;
+    std::vector<double> row(d + 1);
+    amat.resize(amat.size() + (size_t)(d + 1) * (n + 1));  // [a][i]: row a, n+1 columns
+    for (int i = 0; i <= n; ++i) {
+      bary_row_unit(std::cos(pi * i / n), d, row.data());
+      for (int a = 0; a <= d; ++a) amat[amat_off[d] + a * (n + 1) + i] = row[a];
+    }
+  }
+  if (amat.empty()) amat.push_back(0.0);
+  for (int d = 1; d < kMaxNodes; ++d) {
+    ucos_off[d] = (int)ucos.size();
+    for (int i = 0; i <= d; ++i) ucos.push_back(std::cos(pi / d * i));
+  }
+  BTK_TRY(A.upload(&P->d_amat, amat));
+  BTK_TRY(A.upload(&P->d_amat_off, amat_off));
+  BTK_TRY(A.upload(&P->d_ucos, ucos));
+  BTK_TRY(A.upload(&P->d_ucos_off, ucos_off));
+  BTK_TRY(A.upload(&P->d_s_slot_panel, s_panel));
+  BTK_TRY(A.upload(&P->d_s_slot_deg, s_deg));
+  BTK_TRY(A.upload(&P->d_s_slot_off, s_off));
+  BTK_TRY(A.upload(&P->d_s_cluster_slot_begin, s_begin));
+  BTK_TRY(A.upload(&P->d_t_slot_deg, t_deg));
+  BTK_TRY(A.upload(&P->d_t_slot_off, t_off));
+  BTK_TRY(A.upload(&P->d_t_cluster_slot_begin, t_begin));
+  BTK_TRY(A.upload(&P->d_t_cluster_panel, T.clusters));
+
+  // Static items: PP and PC (PC entries start at the degree-n slot).
+  P->n_pc = counts[1];
+  P->n_cp = counts[2];
+  P->n_far = counts[2] + counts[3];
+  std::vector<long long> pc_begin(P->n_pc);
+  std::vector<int> pc_src_cluster(P->n_pc);
+  P->h_pc_tcount.resize(P->n_pc);
+  for (int i = 0; i < P->n_pc; ++i) {
+    const int c = S.cluster_slot[lists[1][i].source_panel];
+    BTK_CHECK(c >= 0, BTK_ERR_INVALID_ARGUMENT, "PC pair with a leaf source");
+    pc_src_cluster[i] = c;
+    pc_begin[i] = S.n_points + s_off[s_begin[c] + (n - dlo)];
+    P->h_pc_tcount[i] = T.h.point_count[lists[1][i].target_panel];
+  }
+  const int counts_static[4] = {counts[0], counts[1], 0, 0};
+  WorkLists W;
+  std::vector<int> pc_entry;
+  BTK_TRY(build_work(T, S, lists, counts_static, slots, W, &pc_begin, &pc_entry));
+  P->evals[0] = W.evals[0];
+  P->n_static_items = (int)W.items.size();
+  P->n_static_entries = (int)W.entries.size();
+  // Far pairs: CP then CC.
+  std::vector<int> far_type(P->n_far), far_tgt(P->n_far), far_src(2 * (size_t)P->n_far);
+  P->h_cp_scount.resize(P->n_cp);
+  for (int i = 0; i < P->n_far; ++i) {
+    const bool cp = i < P->n_cp;
+    const btk_interact_pair& pr = cp ? lists[2][i] : lists[3][i - P->n_cp];
+    BTK_CHECK(pr.target_panel >= 0 && pr.target_panel < T.h.panel_count && pr.source_panel >= 0 &&
+                  pr.source_panel < S.h.panel_count,
+              BTK_ERR_INVALID_ARGUMENT, "interaction list: panel index out of range");
+    far_type[i] = cp ? 2 : 3;
+    far_tgt[i] = T.cluster_slot[pr.target_panel];
+    BTK_CHECK(far_tgt[i] >= 0, BTK_ERR_INVALID_ARGUMENT, "CP/CC pair with a leaf target");
+    if (cp) {
+      BTK_CHECK(S.h.is_leaf[pr.source_panel], BTK_ERR_INVALID_ARGUMENT, "CP pair with a non-leaf source");
+      far_src[2 * i] = S.leaf_begin[pr.source_panel];
+      far_src[2 * i + 1] = S.h.point_count[pr.source_panel];
+      P->h_cp_scount[i] = S.h.point_count[pr.source_panel];
+    } else {
+      far_src[2 * i] = S.cluster_slot[pr.source_panel];
+      BTK_CHECK(far_src[2 * i] >= 0, BTK_ERR_INVALID_ARGUMENT, "CC pair with a leaf source");
+      far_src[2 * i + 1] = 0;
+    }
+  }
+  std::vector<double> centre(3 * (size_t)std::max(nct, 1), 0.0);
+  for (int c = 0; c < nct; ++c)
+    for (int d = 0; d < 3; ++d) {
+      const PanelGeom& g = T.h.geom[T.clusters[c]];
+      centre[3 * c + d] = 0.5 * (g.lo[d] + g.hi[d]);
+    }
+  P->tiles_max = (int)((sz(n) + kTile - 1) / kTile);
+  BTK_TRY(A.upload(&P->d_pc_entry, pc_entry));
+  BTK_TRY(A.upload(&P->d_pc_src_cluster, pc_src_cluster));
+  BTK_TRY(A.upload(&P->d_far_type, far_type));
+  BTK_TRY(A.upload(&P->d_far_tgt, far_tgt));
+  BTK_TRY(A.upload(&P->d_far_src, far_src));
+  BTK_TRY(A.upload(&P->d_tgt_centre, centre));
+  const size_t n_items = (size_t)P->n_static_items + (size_t)P->n_far * P->tiles_max;
+  BTK_CHECK(n_items < (1u << 31), BTK_ERR_UNSUPPORTED, "too many work items");
+  BTK_TRY(A.alloc(&P->ictx.d_items, std::max<size_t>(n_items, 1)));
+  BTK_TRY(A.alloc(&P->ictx.d_entries, std::max<size_t>((size_t)P->n_static_entries + P->n_far, 1)));
+  if (!W.items.empty())
+    BTK_CUDA(cudaMemcpyAsync(P->ictx.d_items, W.items.data(), sizeof(WorkItem) * W.items.size(),
+                             cudaMemcpyHostToDevice, st));
+  if (!W.entries.empty())
+    BTK_CUDA(cudaMemcpyAsync(P->ictx.d_entries, W.entries.data(), sizeof(Entry) * W.entries.size(),
+                             cudaMemcpyHostToDevice, st));
+  P->ictx.n_items = (int)n_items;
+  // Degrees in force: all at n until set.
+  P->h_deg_pc.assign(P->n_pc, n);
+  P->h_deg_far.assign(P->n_far, n);
+  BTK_TRY(A.upload(&P->d_deg_pc, P->h_deg_pc));
+  BTK_TRY(A.upload(&P->d_deg_far, P->h_deg_far));
+  recount_far_evals(P);
+  // Work arrays.
+  BTK_TRY(A.alloc(&P->d_S4, (size_t)S.n_points + P->total_src_slots + 1));
+  BTK_TRY(A.alloc(&P->d_T4, (size_t)T.n_points + P->total_tgt_slots + 1));
+  BTK_TRY(A.alloc(&P->d_T_out, (size_t)T.n_points + P->total_tgt_slots + 1));
+  BTK_TRY(A.alloc(&P->d_ptwm, (size_t)P->ncomp * P->total_tgt_slots + 1));
+  if (T.n_points)
+    BTK_CUDA(cudaMemcpyAsync(P->d_T_out, T.d_perm, sizeof(int) * T.n_points, cudaMemcpyDeviceToDevice, st));
+  std::vector<int> t_slot_panel_dev(t_panel);
+  int* d_t_slot_panel = nullptr;
+  BTK_TRY(A.upload(&d_t_slot_panel, t_slot_panel_dev));
+  BTK_CUDA(launch_tgt_slots(dim, P->n_tgt_slots, d_t_slot_panel, P->d_t_slot_deg, P->d_t_slot_off, T.d_panels,
+                            P->d_ucos, P->d_ucos_off, P->d_T4, P->d_T_out, T.n_points, st));
+  return BTK_OK;
+}
 
 btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
   const btk_run_config& cfg = D->cfg;
@@ -504,30 +722,37 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
                                         "plan: missing interaction list");
   const bool guard = P->eps * P->eps < 1.1754943508222875e-38;
   const int slots = num_sms() * std::max(1, interact_blocks_per_sm(P->dim, P->kind, P->precision, guard));
-  WorkLists W;
-  BTK_TRY(build_work(T, S, lists, counts, slots, W));
-  for (int t = 0; t < 4; ++t) P->evals[t] = W.evals[t];
   P->ictx.dim = P->dim;
   P->ictx.kind = P->kind;
   P->ictx.precision = P->precision;
   P->ictx.eps = P->eps;
-  P->ictx.n_items = (int)W.items.size();
-  BTK_TRY(A.upload(&P->ictx.d_items, W.items));
-  BTK_TRY(A.upload(&P->ictx.d_entries, W.entries));
   BTK_TRY(A.alloc(&P->d_ticket_status, 2));
   BTK_CUDA(cudaMemsetAsync(P->d_ticket_status, 0, 2 * sizeof(int), st));
   P->ictx.d_ticket_status = P->d_ticket_status;
-
-  // Work arrays.
-  BTK_TRY(A.alloc(&P->d_S4, (size_t)S.n_points + (size_t)ncs * P->ipc));
-  BTK_TRY(A.alloc(&P->d_T4, (size_t)T.n_points + (size_t)nct * P->ipc));
-  BTK_TRY(A.alloc(&P->d_T_out, (size_t)T.n_points + (size_t)nct * P->ipc));
   BTK_TRY(A.alloc(&P->d_psw, (size_t)Ps * P->ipc));
   BTK_TRY(A.alloc(&P->d_ptw, (size_t)P->ncomp * Pt * P->ipc));
-  if (T.n_points)
-    BTK_CUDA(cudaMemcpyAsync(P->d_T_out, T.d_perm, sizeof(int) * T.n_points, cudaMemcpyDeviceToDevice, st));
-  BTK_CUDA(launch_tgt_proxies(P->dim, P->degree, nct, T.d_clusters, T.d_nodes_shift, P->d_T4 + T.n_points,
-                              P->d_T_out + T.n_points, st));
+  P->degree_mode = D->degree_mode;
+  P->degree_min = D->degree_min;
+  BTK_CHECK(D->degree_mode == BTK_DEGREE_FIXED || D->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT,
+            "bad degree_mode");
+
+  if (D->degree_mode == BTK_DEGREE_FIXED) {
+    WorkLists W;
+    BTK_TRY(build_work(T, S, lists, counts, slots, W));
+    for (int t = 0; t < 4; ++t) P->evals[t] = W.evals[t];
+    P->ictx.n_items = (int)W.items.size();
+    BTK_TRY(A.upload(&P->ictx.d_items, W.items));
+    BTK_TRY(A.upload(&P->ictx.d_entries, W.entries));
+    BTK_TRY(A.alloc(&P->d_S4, (size_t)S.n_points + (size_t)ncs * P->ipc));
+    BTK_TRY(A.alloc(&P->d_T4, (size_t)T.n_points + (size_t)nct * P->ipc));
+    BTK_TRY(A.alloc(&P->d_T_out, (size_t)T.n_points + (size_t)nct * P->ipc));
+    if (T.n_points)
+      BTK_CUDA(cudaMemcpyAsync(P->d_T_out, T.d_perm, sizeof(int) * T.n_points, cudaMemcpyDeviceToDevice, st));
+    BTK_CUDA(launch_tgt_proxies(P->dim, P->degree, nct, T.d_clusters, T.d_nodes_shift, P->d_T4 + T.n_points,
+                                P->d_T_out + T.n_points, st));
+  } else {
+    BTK_TRY(plan_build_per_pair(P, lists, counts, slots, st));
+  }
   for (int i = 0; i < 6; ++i) BTK_CUDA(cudaEventCreate(&P->ev[i]));
   BTK_CUDA(cudaStreamSynchronize(st));
   return BTK_OK;
@@ -607,27 +832,71 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
   BTK_CUDA(launch_gather(S.n_points, S.d_perm, xs, ys, P->dim == 3 ? zs : nullptr, charges, P->d_S4, st));
   BTK_CUDA(cudaMemsetAsync(P->d_psw, 0, sizeof(double) * (size_t)S.h.panel_count * P->ipc, st));
   BTK_TRY(run_upward(S, P->d_S4, P->d_psw, st));
-  BTK_CUDA(launch_src_proxies(P->dim, P->degree, (int)S.clusters.size(), S.d_clusters, S.d_nodes_shift, P->d_psw,
+  const bool per_pair = P->degree_mode == BTK_DEGREE_PER_PAIR;
+  if (!per_pair) {
+    BTK_CUDA(launch_src_proxies(P->dim, P->degree, (int)S.clusters.size(), S.d_clusters, S.d_nodes_shift, P->d_psw,
+                                P->d_S4 + S.n_points, st));
+  } else {
+    // Every source cluster at every slot degree, then the work items for the
+    // degrees in force.
+    BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
+                              S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
                               P->d_S4 + S.n_points, st));
+    BTK_CUDA(launch_resolve(P->dim, P->n_pc, P->d_pc_entry, P->d_pc_src_cluster, P->d_deg_pc, P->n_far, P->tiles_max,
+                            P->d_far_type, P->d_far_tgt, P->d_far_src, P->d_deg_far, P->d_s_slot_off,
+                            P->d_s_cluster_slot_begin, P->d_t_slot_off, P->d_t_cluster_slot_begin, P->degree_min,
+                            T.n_points, S.n_points, P->d_tgt_centre, P->n_static_items, P->ictx.d_items,
+                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, st));
+  }
   BTK_CUDA(cudaEventRecord(P->ev[1], st));
   // Interactions.
   BTK_CUDA(launch_gather(T.n_points, T.d_perm, xt, yt, P->dim == 3 ? zt : nullptr, nullptr, P->d_T4, st));
   BTK_CUDA(cudaMemsetAsync(P->d_ptw, 0, sizeof(double) * (size_t)P->ncomp * Pt * P->ipc, st));
   BTK_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)P->ncomp * T.n_points, st));
-  Ptr4 o{}, w{};
+  Ptr4 o{}, w{}, wm{};
   for (int c = 0; c < P->ncomp; ++c) {
     o.p[c] = out + (size_t)c * T.n_points;
     w.p[c] = P->d_ptw + (size_t)c * Pt * P->ipc;
+    if (per_pair) wm.p[c] = P->d_ptwm + (size_t)c * P->total_tgt_slots;
   }
+  if (per_pair) BTK_CUDA(cudaMemsetAsync(P->d_ptwm, 0, sizeof(double) * (size_t)P->ncomp * P->total_tgt_slots, st));
   // The kernel-tight pair is recorded only when there is a launch to bracket.
   BTK_CUDA(cudaEventRecord(P->ev[4], st));
   BTK_CUDA(cudaEventRecord(P->ev[5], st));
-  BTK_TRY(run_interactions(P->ictx, P->d_S4, P->d_T4, P->d_T_out, o, w, st, P->ev[4], P->ev[5]));
+  BTK_TRY(run_interactions(P->ictx, P->d_S4, P->d_T4, P->d_T_out, o, per_pair ? wm : w, st, P->ev[4], P->ev[5]));
+  if (per_pair)
+    BTK_CUDA(launch_promote(P->dim, P->degree, P->ncomp, (int)T.clusters.size(), P->d_t_cluster_panel,
+                            P->d_t_cluster_slot_begin, P->d_t_slot_deg, P->d_t_slot_off, P->d_amat, P->d_amat_off,
+                            wm, w, st));
   BTK_CUDA(cudaEventRecord(P->ev[2], st));
   // Downward.
   BTK_TRY(run_downward(T, P->ncomp, P->d_T4, w, o, st));
   BTK_CUDA(cudaEventRecord(P->ev[3], st));
   P->timed = true;
+  return BTK_OK;
+}
+
+btk_status btk_plan_set_degrees(btk_plan* P, const int* deg_pc, const int* deg_cp, const int* deg_cc) {
+  BTK_CHECK(P, BTK_ERR_INVALID_ARGUMENT, "null plan");
+  BTK_CHECK(P->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT, "plan is not BTK_DEGREE_PER_PAIR");
+  const int lo = P->degree_min, hi = P->degree;
+  auto check = [&](const int* v, int n) {
+    for (int i = 0; i < n; ++i)
+      if (v[i] < lo || v[i] > hi) return false;
+    return true;
+  };
+  const int n_cc = P->n_far - P->n_cp;
+  BTK_CHECK(!deg_pc || check(deg_pc, P->n_pc), BTK_ERR_INVALID_ARGUMENT, "PC degree outside [degree_min, degree]");
+  BTK_CHECK(!deg_cp || check(deg_cp, P->n_cp), BTK_ERR_INVALID_ARGUMENT, "CP degree outside [degree_min, degree]");
+  BTK_CHECK(!deg_cc || check(deg_cc, n_cc), BTK_ERR_INVALID_ARGUMENT, "CC degree outside [degree_min, degree]");
+  if (deg_pc) std::copy(deg_pc, deg_pc + P->n_pc, P->h_deg_pc.begin());
+  if (deg_cp) std::copy(deg_cp, deg_cp + P->n_cp, P->h_deg_far.begin());
+  if (deg_cc) std::copy(deg_cc, deg_cc + n_cc, P->h_deg_far.begin() + P->n_cp);
+  BTK_CUDA(cudaMemcpyAsync(P->d_deg_pc, P->h_deg_pc.data(), sizeof(int) * P->n_pc, cudaMemcpyHostToDevice, P->stream));
+  BTK_CUDA(cudaMemcpyAsync(P->d_deg_far, P->h_deg_far.data(), sizeof(int) * P->n_far, cudaMemcpyHostToDevice,
+                           P->stream));
+  BTK_CUDA(cudaStreamSynchronize(P->stream));
+  recount_far_evals(P);
   return BTK_OK;
 }
 

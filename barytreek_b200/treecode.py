@@ -143,11 +143,12 @@ class Treecode:
     """
 
     def __init__(self, coords, sources=None, *, degree=8, cluster_size=100, theta=0.7, eps=1e-4, kind=KIND_POT,
-                 precision=PREC_FP64, device="cuda"):
+                 precision=PREC_FP64, degree_mode=_lib.DEGREE_FIXED, degree_min=1, device="cuda"):
         import torch
 
         self.dim = len(coords)
         self.kind, self.precision = kind, precision
+        self.degree_mode, self.degree_min = degree_mode, degree_min
         self.ncomp = ncomp(self.dim, kind)
         self.cfg = make_run_config(self.dim, degree, cluster_size, theta, eps)
         self.targets = tuple(np.ascontiguousarray(c, np.float64) for c in coords)
@@ -184,8 +185,14 @@ class Treecode:
         d.point_leaf_panel_source = ptr(src.point_leaf_panel)
         d.pp_list, d.pc_list, d.cp_list, d.cc_list = [ptr(l) if len(l) else None for l in self.lists]
         d.kind, d.precision = self.kind, self.precision
+        d.degree_mode, d.degree_min = self.degree_mode, self.degree_min
         stream = torch.cuda.current_stream(self.device).cuda_stream
         check(load().btk_plan_create(ctypes.byref(self._plan), ctypes.byref(d), stream))
+
+    def set_degrees(self, deg_pc=None, deg_cp=None, deg_cc=None):
+        """Per-pair degrees for a degree_mode=DEGREE_PER_PAIR plan (host arrays in list order)."""
+        arrs = [None if d is None else np.ascontiguousarray(d, np.int32) for d in (deg_pc, deg_cp, deg_cc)]
+        check(load().btk_plan_set_degrees(self._plan, *[ptr(a) for a in arrs]))
 
     def stats(self) -> dict:
         s = _lib.PlanStats()

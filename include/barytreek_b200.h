@@ -268,7 +268,22 @@ typedef struct {
   const btk_interact_pair* cc_list;
   int kind;      /* btk_kind */
   int precision; /* btk_precision */
+  /* BTK_DEGREE_FIXED: every interaction at cfg.interp_degree (the reference
+   * method). BTK_DEGREE_PER_PAIR: each PC/CP/CC pair at its own degree in
+   * [degree_min, cfg.interp_degree], set with btk_plan_set_degrees or chosen by
+   * the learned selector; the upward/downward passes stay at
+   * cfg.interp_degree (exact anterpolation/promotion between degrees). */
+  int degree_mode;
+  int degree_min;
 } btk_plan_desc;
+
+enum { BTK_DEGREE_FIXED = 0, BTK_DEGREE_PER_PAIR = 1 };
+
+/* Per-pair degrees (host arrays, one entry per pair of the plan's PC, CP and
+ * CC lists, in list order; NULL keeps a class at its current degrees). Only for
+ * BTK_DEGREE_PER_PAIR plans; values outside [degree_min, interp_degree] are
+ * rejected. */
+btk_status btk_plan_set_degrees(btk_plan* plan, const int* deg_pc, const int* deg_cp, const int* deg_cc);
 
 btk_status btk_plan_create(btk_plan** plan, const btk_plan_desc* desc, btk_stream_t stream);
 btk_status btk_plan_destroy(btk_plan* plan);
