@@ -108,9 +108,27 @@ SIGNATURES = {
     "btk_solve_host": [_ci, _ci, _ci, _ci, _ci, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_measure_pipe_peak": [_ci, _vp, _vp],
     "btk_plan_set_degrees": [_vp, _vp, _vp, _vp],
+    "btk_selector_param_count": [],
+    "btk_selector_create": [_vp, _vp, _vp],
+    "btk_selector_destroy": [_vp],
+    "btk_selector_weights": [_vp],
+    "btk_plan_pair_count": [_vp, _vp],
+    "btk_plan_pair_features": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "btk_plan_execute_learned": [_vp, _vp, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "btk_plan_error_samples": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _ci, _vp, _ci, _vp, _vp, _vp, _vp, _vp],
+    "btk_mlp_forward": [_vp, _ci, _vp, _vp, _vp],
+    "btk_mlp_gradient": [_vp, _ci, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "btk_mlp_adam": [_vp, _vp, _vp, _vp, _vp, _ci, ctypes.c_float, _vp],
 }
 _RESTYPES = {"btk_last_error": ctypes.c_char_p, "btk_version": ctypes.c_char_p, "btk_launch_count": ctypes.c_uint64,
-             "btk_free": None}
+             "btk_free": None, "btk_selector_weights": ctypes.c_void_p}
+
+
+class LearnedReport(ctypes.Structure):
+    """btk_learned_report."""
+    _fields_ = [("audit_rel_l2", ctypes.c_double), ("audit_targets", ctypes.c_int), ("fell_back", ctypes.c_int),
+                ("evals_near", ctypes.c_int64), ("evals_far", ctypes.c_int64), ("ms_select", ctypes.c_float),
+                ("ms_solve", ctypes.c_float), ("ms_total", ctypes.c_float), ("degree_hist", ctypes.c_int * 13)]
 
 _lib = None
 

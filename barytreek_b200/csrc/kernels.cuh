@@ -105,6 +105,53 @@ int interact_blocks_per_sm(int dim, int kind, int precision, bool guard);
 cudaError_t launch_direct(int dim, int kind, double eps, int nt, const double* xt, const double* yt,
                           const double* zt, int ns, const double4* src, double* out, cudaStream_t s);
 
+// ---- learned selector (selector.cu) -------------------------------------------
+// Inputs of the training-sample generator (see btk_plan_error_samples).
+struct SampleArgs {
+  int dim, kind, ncomp, K, n_deg, deg_lo, n;
+  double eps2;
+  const int* pair_index;  // [n] into the plan's pair list
+  const int* ptype;       // per pair: 1 PC, 2 CP, 3 CC
+  const int* ptgt;        // per pair target panel
+  const int* psrc;        // per pair source panel
+  const double* xt;
+  const double* yt;
+  const double* zt;
+  const int* tgt_orig;  // [n][K] original target indices
+  const int* src_leaf_csr;
+  const int* src_leaves;  // leaf panels under each sample's source
+  const int* leaf_begin_s;
+  const int* count_s;
+  const double4* S4;       // sorted source points then source slots
+  const long long* s_slot_off;
+  const int* s_slot_begin;  // per source cluster slot index
+  const int* cluster_slot_s;
+  const double4* T4;  // target slots after the points
+  const long long* t_slot_off;
+  const int* t_slot_begin;
+  const int* cluster_slot_t;
+  long long ns, nt;
+  const DevPanel* pt;
+  int slot_d_lo;
+  double* exact;   // [n][K][ncomp]
+  double* approx;  // [n][n_deg][K][ncomp]
+};
+cudaError_t launch_error_samples(const SampleArgs& a, float* log10_err, cudaStream_t s);
+int selector_param_count();
+cudaError_t launch_panel_desc(int dim, int n, int P, const double* psw, float* desc, cudaStream_t s);
+cudaError_t launch_pair_features(int n_pairs, const int* ptype, const int* ptgt, const int* psrc, const DevPanel* pt,
+                                 const DevPanel* ps, double root_radius, double eps, const float* desc_s, float* feat,
+                                 cudaStream_t s);
+cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const float* feat, float* out,
+                             cudaStream_t s);
+cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int* deg,
+                                  cudaStream_t s);
+cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
+                             const int* cp_scount, unsigned long long* evals, cudaStream_t s);
+cudaError_t launch_audit_compare(int n, int ncomp, int nt, const int* audit_sorted, const int* perm,
+                                 const double* out, const double* audit_out, double* sums, cudaStream_t s);
+cudaError_t launch_fill_int(int n, int value, int* dst, cudaStream_t s);
+
 // ---- per-pair degrees (kernels_degree.cu) -------------------------------------
 cudaError_t launch_src_slots(int dim, int n, int n_slots, const int* slot_cluster_panel, const int* slot_degree,
                              const long long* slot_offset, const DevPanel* panels, const double* psw,

@@ -248,13 +248,30 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
   std::vector<Entry> grouped(head[Pt]);
   std::vector<int> cur(head.begin(), head.end() - 1);
   std::vector<int> n_near(Pt, 0);  // PP entries lead each target's group
+  std::vector<char> touching(head[Pt], 0);
   std::vector<int> final_index(head[Pt], -1);
   if (pc_entry) pc_entry->assign(counts[1], -1);
+  // A PP source leaf "touches" the target leaf when the gap between the boxes
+  // is under half the target's smallest side. Only such pairs can be far
+  // closer than their distance to the item's centre, so only their sources
+  // take the mixed kernel's hi/lo coordinate path.
+  auto touches = [&](int tp, int sp) {
+    const PanelGeom &a = T.h.geom[tp], &b = S.h.geom[sp];
+    double gap = 0.0, side = 1e300;
+    for (int d = 0; d < T.h.dim; ++d) {
+      gap = std::max(gap, std::max(b.lo[d] - a.hi[d], a.lo[d] - b.hi[d]));
+      side = std::min(side, a.hi[d] - a.lo[d]);
+    }
+    return gap <= 0.5 * side;
+  };
   for (int t = 0; t < 4; ++t)
     for (int i = 0; i < counts[t]; ++i) {
       const btk_interact_pair& pr = lists[t][i];
       const int sp = pr.source_panel, tp = pr.target_panel;
-      if (t == 0) n_near[tp]++;
+      if (t == 0) {
+        n_near[tp]++;
+        touching[cur[tp]] = touches(tp, sp);
+      }
       Entry e;
       if (t & 1) {  // cluster source: its proxies
         e.s_begin = (t == 1 && pc_begin) ? (int)(*pc_begin)[i] : ns + S.cluster_slot[sp] * ipc;
@@ -277,6 +294,18 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
     const int eb = head[tp], ee = head[tp + 1];
     if (eb == ee) continue;
     const int e0 = (int)W.entries.size();
+    // Touching PP sources first (stable), then the other PP sources, then PC.
+    int n_touch = 0;
+    {
+      std::vector<Entry> seg;
+      seg.reserve(n_near[tp]);
+      for (int k = eb; k < eb + n_near[tp]; ++k)
+        if (touching[k]) seg.push_back(grouped[k]);
+      n_touch = (int)seg.size();
+      for (int k = eb; k < eb + n_near[tp]; ++k)
+        if (!touching[k]) seg.push_back(grouped[k]);
+      std::copy(seg.begin(), seg.end(), grouped.begin() + eb);
+    }
     int s_total = 0, e_near = e0;
     for (int k = eb; k < ee; ++k) {
       if (grouped[k].s_count > 0) {
@@ -284,7 +313,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
         W.entries.push_back(grouped[k]);
         s_total += grouped[k].s_count;
       }
-      if (k - eb < n_near[tp]) e_near = (int)W.entries.size();
+      if (k - eb < n_touch) e_near = (int)W.entries.size();
     }
     const int e1 = (int)W.entries.size();
     // Sources of entries [kb, ke) that are near-field (PP) points.
@@ -476,6 +505,27 @@ struct btk_plan {
   double* d_ptwm = nullptr;                       // ncomp x total_tgt_slots
   // host copies for work accounting
   std::vector<int> h_pc_tcount, h_cp_scount, h_deg_pc, h_deg_far;
+
+  // ---- learned selector (per-pair plans) ----
+  int n_pairs = 0;  // PC, then CP, then CC
+  int *d_pair_type = nullptr, *d_pair_tgt = nullptr, *d_pair_src = nullptr;
+  int *d_pc_tcount = nullptr, *d_cp_scount = nullptr;
+  float *d_desc = nullptr, *d_feat = nullptr, *d_pred = nullptr;
+  unsigned long long* d_evals = nullptr;
+  int* d_hist = nullptr;
+  double root_radius = 1.0, root_centre[3] = {0, 0, 0};
+  // audit: a fixed 1% sample of the targets, direct sum over all sources
+  int n_audit = 0;
+  int *d_audit_orig = nullptr, *d_audit_tout = nullptr;
+  double4* d_audit_T4 = nullptr;
+  double *d_audit_out = nullptr, *d_audit_sums = nullptr;
+  btk::InteractCtx audit_ctx;
+  int *d_cluster_slot_s = nullptr, *d_cluster_slot_t = nullptr;  // panel -> cluster index (or -1)
+};
+
+struct btk_selector {
+  void* d_w = nullptr;  // BF16 parameters
+  float norm[34] = {};  // feature mean[16], std[16], target mean, std
 };
 
 using namespace btk;
@@ -652,9 +702,51 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   // Degrees in force: all at n until set.
   P->h_deg_pc.assign(P->n_pc, n);
   P->h_deg_far.assign(P->n_far, n);
-  BTK_TRY(A.upload(&P->d_deg_pc, P->h_deg_pc));
-  BTK_TRY(A.upload(&P->d_deg_far, P->h_deg_far));
+  P->n_pairs = P->n_pc + P->n_far;
+  {
+    std::vector<int> all(std::max(P->n_pairs, 1), n);
+    BTK_TRY(A.upload(&P->d_deg_pc, all));  // one array: PC degrees, then CP, then CC
+    P->d_deg_far = P->d_deg_pc + P->n_pc;
+  }
   recount_far_evals(P);
+  // Selector inputs: pair classes and panels (PC, CP, CC), per-pair point counts.
+  {
+    std::vector<int> ty(std::max(P->n_pairs, 1)), tg(std::max(P->n_pairs, 1)), sr(std::max(P->n_pairs, 1));
+    for (int i = 0; i < P->n_pc; ++i) {
+      ty[i] = 1;
+      tg[i] = lists[1][i].target_panel;
+      sr[i] = lists[1][i].source_panel;
+    }
+    for (int i = 0; i < P->n_far; ++i) {
+      const bool cp = i < P->n_cp;
+      const btk_interact_pair& pr = cp ? lists[2][i] : lists[3][i - P->n_cp];
+      ty[P->n_pc + i] = cp ? 2 : 3;
+      tg[P->n_pc + i] = pr.target_panel;
+      sr[P->n_pc + i] = pr.source_panel;
+    }
+    BTK_TRY(A.upload(&P->d_pair_type, ty));
+    BTK_TRY(A.upload(&P->d_pair_tgt, tg));
+    BTK_TRY(A.upload(&P->d_pair_src, sr));
+    std::vector<int> tc(P->h_pc_tcount), sc(P->h_cp_scount);
+    tc.push_back(0);
+    sc.push_back(0);
+    BTK_TRY(A.upload(&P->d_pc_tcount, tc));
+    BTK_TRY(A.upload(&P->d_cp_scount, sc));
+    BTK_TRY(A.alloc(&P->d_desc, (size_t)S.h.panel_count * 6));
+    BTK_TRY(A.alloc(&P->d_feat, (size_t)std::max(P->n_pairs, 1) * 16));
+    BTK_TRY(A.alloc(&P->d_pred, (size_t)std::max(P->n_pairs, 1) * 9));
+    BTK_TRY(A.alloc(&P->d_evals, 1));
+    BTK_TRY(A.alloc(&P->d_hist, kMaxNodes));
+    BTK_TRY(A.upload(&P->d_cluster_slot_s, S.cluster_slot));
+    BTK_TRY(A.upload(&P->d_cluster_slot_t, T.cluster_slot));
+    const PanelGeom& g = S.h.geom[0];
+    double r2 = 0;
+    for (int d = 0; d < dim; ++d) {
+      r2 += (g.hi[d] - g.lo[d]) * (g.hi[d] - g.lo[d]);
+      P->root_centre[d] = 0.5 * (g.lo[d] + g.hi[d]);
+    }
+    P->root_radius = std::max(0.5 * std::sqrt(r2), 1e-300);
+  }
   // Work arrays.
   BTK_TRY(A.alloc(&P->d_S4, (size_t)S.n_points + P->total_src_slots + 1));
   BTK_TRY(A.alloc(&P->d_T4, (size_t)T.n_points + P->total_tgt_slots + 1));
@@ -873,6 +965,317 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
   BTK_TRY(run_downward(T, P->ncomp, P->d_T4, w, o, st));
   BTK_CUDA(cudaEventRecord(P->ev[3], st));
   P->timed = true;
+  return BTK_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// A fixed, seeded 1% sample of the targets (at least one), and work items for
+// the direct sum over every source: tiles of kTile audited targets times
+// pieces of the sorted source points, all sources on the hi/lo path.
+btk_status setup_audit(btk_plan* P, cudaStream_t st) {
+  if (P->n_audit > 0) return BTK_OK;
+  Arena& A = *P->arena;
+  const int nt = P->tgt.n_points, ns = P->src->n_points;
+  const int na = std::max(1, nt / 100);
+  std::vector<int> orig(na);
+  // Evenly spread, seeded offsets (SplitMix64-style hash) over the index range.
+  for (int k = 0; k < na; ++k) {
+    uint64_t z = 0x9E3779B97F4A7C15ULL * (uint64_t)(k + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    const int64_t lo = (int64_t)k * nt / na, hi = (int64_t)(k + 1) * nt / na;
+    orig[k] = (int)(lo + (int64_t)(z % (uint64_t)std::max<int64_t>(1, hi - lo)));
+  }
+  std::vector<int> tout(na);
+  std::iota(tout.begin(), tout.end(), 0);
+  BTK_TRY(A.upload(&P->d_audit_orig, orig));
+  BTK_TRY(A.upload(&P->d_audit_tout, tout));
+  BTK_TRY(A.alloc(&P->d_audit_T4, (size_t)na));
+  BTK_TRY(A.alloc(&P->d_audit_out, (size_t)P->ncomp * na));
+  BTK_TRY(A.alloc(&P->d_audit_sums, 2));
+  const int tiles = (na + kTile - 1) / kTile;
+  const int slots = num_sms() * 6;
+  const int pieces = std::max(1, std::min(ns, (2 * slots + tiles - 1) / tiles));
+  std::vector<Entry> entries;
+  std::vector<WorkItem> items;
+  for (int p = 0; p < pieces; ++p) {
+    const int b = (int)((int64_t)p * ns / pieces), e = (int)((int64_t)(p + 1) * ns / pieces);
+    if (e > b) entries.push_back(Entry{b, e - b});
+  }
+  for (int t = 0; t < tiles; ++t)
+    for (int p = 0; p < (int)entries.size(); ++p) {
+      WorkItem w{};
+      w.t_begin = t * kTile;
+      w.t_count = std::min(kTile, na - t * kTile);
+      w.e_begin = p;
+      w.e_end = p + 1;
+      w.s_total = entries[p].s_count;
+      w.flags = kItemAtomic;
+      w.near_total = w.s_total;
+      w.cx = P->root_centre[0];
+      w.cy = P->root_centre[1];
+      w.cz = P->root_centre[2];
+      items.push_back(w);
+    }
+  P->audit_ctx = P->ictx;
+  P->audit_ctx.n_items = (int)items.size();
+  BTK_TRY(A.upload(&P->audit_ctx.d_items, items));
+  BTK_TRY(A.upload(&P->audit_ctx.d_entries, entries));
+  BTK_TRY(A.alloc(&P->audit_ctx.d_ticket_status, 2));
+  BTK_CUDA(cudaMemsetAsync(P->audit_ctx.d_ticket_status, 0, 2 * sizeof(int), st));
+  P->n_audit = na;
+  return BTK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+btk_status btk_selector_create(btk_selector** out, const float* params, const float* norm) {
+  BTK_CHECK(out && params && norm, BTK_ERR_INVALID_ARGUMENT, "btk_selector_create: null argument");
+  const int np = selector_param_count();
+  std::vector<uint16_t> bf(np);
+  for (int i = 0; i < np; ++i) {  // round to nearest even BF16
+    uint32_t u;
+    std::memcpy(&u, &params[i], 4);
+    const uint32_t lsb = (u >> 16) & 1u;
+    u += 0x7FFFu + lsb;
+    bf[i] = (uint16_t)(u >> 16);
+  }
+  btk_selector* s = new btk_selector();
+  std::memcpy(s->norm, norm, sizeof(s->norm));
+  cudaError_t e = cudaMalloc(&s->d_w, sizeof(uint16_t) * np);
+  if (e == cudaSuccess) e = cudaMemcpy(s->d_w, bf.data(), sizeof(uint16_t) * np, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(s->d_w);
+    delete s;
+    return cuda_error(e, "btk_selector_create");
+  }
+  *out = s;
+  return BTK_OK;
+}
+
+btk_status btk_selector_destroy(btk_selector* s) {
+  if (!s) return BTK_OK;
+  cudaFree(s->d_w);
+  delete s;
+  return BTK_OK;
+}
+
+const void* btk_selector_weights(const btk_selector* s) { return s ? s->d_w : nullptr; }
+
+btk_status btk_plan_pair_count(const btk_plan* P, int* n_pairs) {
+  BTK_CHECK(P && n_pairs, BTK_ERR_INVALID_ARGUMENT, "null argument");
+  BTK_CHECK(P->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT, "plan is not BTK_DEGREE_PER_PAIR");
+  *n_pairs = P->n_pairs;
+  return BTK_OK;
+}
+
+// Upward pass, panel descriptors and far-pair features for the given charges.
+btk_status btk_plan_pair_features(btk_plan* P, const double* xs, const double* ys, const double* zs,
+                                  const double* charges, float* features, btk_stream_t stream) {
+  BTK_CHECK(P && xs && ys && charges && features && (P->dim == 2 || zs), BTK_ERR_INVALID_ARGUMENT,
+            "btk_plan_pair_features: null argument");
+  BTK_CHECK(P->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT, "plan is not BTK_DEGREE_PER_PAIR");
+  cudaStream_t st = (cudaStream_t)stream;
+  Side& S = *P->src;
+  BTK_CUDA(launch_gather(S.n_points, S.d_perm, xs, ys, P->dim == 3 ? zs : nullptr, charges, P->d_S4, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_psw, 0, sizeof(double) * (size_t)S.h.panel_count * P->ipc, st));
+  BTK_TRY(run_upward(S, P->d_S4, P->d_psw, st));
+  BTK_CUDA(launch_panel_desc(P->dim, P->degree, S.h.panel_count, P->d_psw, P->d_desc, st));
+  BTK_CUDA(launch_pair_features(P->n_pairs, P->d_pair_type, P->d_pair_tgt, P->d_pair_src, P->tgt.d_panels,
+                                S.d_panels, P->root_radius, P->eps, P->d_desc, features, st));
+  return BTK_OK;
+}
+
+btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double tol, double pair_tol, int degree_lo,
+                                    const double* xt, const double* yt, const double* zt, const double* xs,
+                                    const double* ys, const double* zs, const double* charges, double* out,
+                                    btk_learned_report* report, btk_stream_t stream) {
+  BTK_CHECK(P && sel && xt && yt && xs && ys && charges && out && (P->dim == 2 || (zt && zs)),
+            BTK_ERR_INVALID_ARGUMENT, "btk_plan_execute_learned: null argument");
+  BTK_CHECK(P->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT, "plan is not BTK_DEGREE_PER_PAIR");
+  BTK_CHECK(tol > 0 && pair_tol > 0, BTK_ERR_INVALID_ARGUMENT, "tolerances must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  Side& T = P->tgt;
+  Side& S = *P->src;
+  const int Pt = T.h.panel_count;
+  BTK_TRY(setup_audit(P, st));
+  cudaEvent_t e[4];
+  for (auto& x : e) BTK_CUDA(cudaEventCreate(&x));
+  BTK_CUDA(cudaEventRecord(e[0], st));
+  // Upward pass and features, then the selector's degrees.
+  BTK_TRY(btk_plan_pair_features(P, xs, ys, zs, charges, P->d_feat, stream));
+  BTK_CUDA(launch_mlp_infer(P->n_pairs, sel->d_w, sel->norm, P->d_feat, P->d_pred, st));
+  const int lo = std::max(std::max(degree_lo, P->degree_min), 1);
+  BTK_CUDA(launch_choose_degrees(P->n_pairs, P->d_pred, (float)std::log10(pair_tol), lo, P->degree, P->d_deg_pc, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_evals, 0, sizeof(unsigned long long), st));
+  BTK_CUDA(cudaMemsetAsync(P->d_hist, 0, sizeof(int) * kMaxNodes, st));
+  BTK_CUDA(launch_far_evals(P->dim, P->n_pc, P->n_cp, P->n_far - P->n_cp, P->d_deg_pc, P->d_pc_tcount,
+                            P->d_cp_scount, P->d_evals, st));
+  BTK_CUDA(cudaEventRecord(e[1], st));
+  // Solve at the chosen degrees.
+  Ptr4 o{}, w{}, wm{};
+  for (int c = 0; c < P->ncomp; ++c) {
+    o.p[c] = out + (size_t)c * T.n_points;
+    w.p[c] = P->d_ptw + (size_t)c * Pt * P->ipc;
+    wm.p[c] = P->d_ptwm + (size_t)c * P->total_tgt_slots;
+  }
+  auto solve = [&](const InteractCtx& ctx) -> btk_status {
+    BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
+                              S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
+                              P->d_S4 + S.n_points, st));
+    BTK_CUDA(launch_resolve(P->dim, P->n_pc, P->d_pc_entry, P->d_pc_src_cluster, P->d_deg_pc, P->n_far, P->tiles_max,
+                            P->d_far_type, P->d_far_tgt, P->d_far_src, P->d_deg_far, P->d_s_slot_off,
+                            P->d_s_cluster_slot_begin, P->d_t_slot_off, P->d_t_cluster_slot_begin, P->degree_min,
+                            T.n_points, S.n_points, P->d_tgt_centre, P->n_static_items, P->ictx.d_items,
+                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, st));
+    BTK_CUDA(launch_gather(T.n_points, T.d_perm, xt, yt, P->dim == 3 ? zt : nullptr, nullptr, P->d_T4, st));
+    BTK_CUDA(cudaMemsetAsync(P->d_ptw, 0, sizeof(double) * (size_t)P->ncomp * Pt * P->ipc, st));
+    BTK_CUDA(cudaMemsetAsync(P->d_ptwm, 0, sizeof(double) * (size_t)P->ncomp * P->total_tgt_slots, st));
+    BTK_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)P->ncomp * T.n_points, st));
+    BTK_TRY(run_interactions(ctx, P->d_S4, P->d_T4, P->d_T_out, o, wm, st));
+    BTK_CUDA(launch_promote(P->dim, P->degree, P->ncomp, (int)T.clusters.size(), P->d_t_cluster_panel,
+                            P->d_t_cluster_slot_begin, P->d_t_slot_deg, P->d_t_slot_off, P->d_amat, P->d_amat_off,
+                            wm, w, st));
+    BTK_TRY(run_downward(T, P->ncomp, P->d_T4, w, o, st));
+    return BTK_OK;
+  };
+  BTK_TRY(solve(P->ictx));
+  BTK_CUDA(cudaEventRecord(e[2], st));
+  // Audit: direct sum at the sampled targets.
+  BTK_CUDA(launch_gather(P->n_audit, P->d_audit_orig, xt, yt, P->dim == 3 ? zt : nullptr, nullptr, P->d_audit_T4, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_audit_out, 0, sizeof(double) * (size_t)P->ncomp * P->n_audit, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_audit_sums, 0, 2 * sizeof(double), st));
+  Ptr4 ao{};
+  for (int c = 0; c < P->ncomp; ++c) ao.p[c] = P->d_audit_out + (size_t)c * P->n_audit;
+  BTK_TRY(run_interactions(P->audit_ctx, P->d_S4, P->d_audit_T4, P->d_audit_tout, ao, ao, st));
+  BTK_CUDA(launch_audit_compare(P->n_audit, P->ncomp, T.n_points, P->d_audit_orig, nullptr, out, P->d_audit_out,
+                                P->d_audit_sums, st));
+  double sums[2] = {0, 0};
+  unsigned long long ev = 0;
+  BTK_CUDA(cudaMemcpyAsync(sums, P->d_audit_sums, sizeof(sums), cudaMemcpyDeviceToHost, st));
+  BTK_CUDA(cudaMemcpyAsync(&ev, P->d_evals, sizeof(ev), cudaMemcpyDeviceToHost, st));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  const double rel = std::sqrt(sums[0] / std::max(sums[1], 1e-300));
+  int hist[13] = {0};
+  if (report && P->n_pairs) {  // degrees the selector chose (before any fallback)
+    std::vector<int> deg(P->n_pairs);
+    BTK_CUDA(cudaMemcpy(deg.data(), P->d_deg_pc, sizeof(int) * P->n_pairs, cudaMemcpyDeviceToHost));
+    for (int d : deg)
+      if (d >= 0 && d < 13) hist[d]++;
+  }
+  int fell_back = 0;
+  if (!(rel <= tol)) {
+    // Fallback: the fixed-degree plain method (degree n everywhere, FP64).
+    fell_back = 1;
+    BTK_CUDA(launch_fill_int(P->n_pairs, P->degree, P->d_deg_pc, st));
+    InteractCtx plain = P->ictx;
+    plain.precision = BTK_PREC_FP64;
+    BTK_TRY(solve(plain));
+  }
+  BTK_CUDA(cudaEventRecord(e[3], st));
+  BTK_CUDA(cudaEventSynchronize(e[3]));
+  if (report) {
+    std::memset(report, 0, sizeof(*report));
+    report->audit_rel_l2 = rel;
+    report->audit_targets = P->n_audit;
+    report->fell_back = fell_back;
+    report->evals_far = (int64_t)ev;
+    report->evals_near = P->evals[0];
+    cudaEventElapsedTime(&report->ms_select, e[0], e[1]);
+    cudaEventElapsedTime(&report->ms_solve, e[1], e[2]);
+    cudaEventElapsedTime(&report->ms_total, e[0], e[3]);
+    std::memcpy(report->degree_hist, hist, sizeof(hist));
+  }
+  for (auto& x : e) cudaEventDestroy(x);
+  return check_status_word(P->ictx.d_ticket_status + 1, st);
+}
+
+btk_status btk_plan_error_samples(btk_plan* P, const double* xt, const double* yt, const double* zt,
+                                  const double* xs, const double* ys, const double* zs, const double* charges, int n,
+                                  const int* pair_index, int K, const int* target_orig, const int* src_leaf_csr,
+                                  const int* src_leaves, float* log10_err, btk_stream_t stream) {
+  BTK_CHECK(P && xt && yt && xs && ys && charges && (P->dim == 2 || (zt && zs)), BTK_ERR_INVALID_ARGUMENT,
+            "btk_plan_error_samples: null argument");
+  BTK_CHECK(P->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT, "plan is not BTK_DEGREE_PER_PAIR");
+  BTK_CHECK(n >= 0 && K >= 1 && K <= 128 && (n == 0 || (pair_index && target_orig && src_leaf_csr && src_leaves &&
+                                                        log10_err)),
+            BTK_ERR_INVALID_ARGUMENT, "btk_plan_error_samples: bad sample arrays (1 <= K <= 128)");
+  if (n == 0) return BTK_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  Side& T = P->tgt;
+  Side& S = *P->src;
+  for (int i = 0; i < n; ++i) {
+    BTK_CHECK(pair_index[i] >= 0 && pair_index[i] < P->n_pairs, BTK_ERR_INVALID_ARGUMENT, "sample pair out of range");
+    BTK_CHECK(src_leaf_csr[i + 1] >= src_leaf_csr[i], BTK_ERR_INVALID_ARGUMENT, "bad source leaf CSR");
+  }
+  for (int i = 0; i < n * K; ++i)
+    BTK_CHECK(target_orig[i] >= 0 && target_orig[i] < T.n_points, BTK_ERR_INVALID_ARGUMENT, "sample target out of range");
+  for (int i = 0; i < src_leaf_csr[n]; ++i)
+    BTK_CHECK(src_leaves[i] >= 0 && src_leaves[i] < S.h.panel_count && S.h.is_leaf[src_leaves[i]],
+              BTK_ERR_INVALID_ARGUMENT, "sample source leaf is not a leaf panel");
+  // Sources and all degree slots for these charges.
+  BTK_CUDA(launch_gather(S.n_points, S.d_perm, xs, ys, P->dim == 3 ? zs : nullptr, charges, P->d_S4, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_psw, 0, sizeof(double) * (size_t)S.h.panel_count * P->ipc, st));
+  BTK_TRY(run_upward(S, P->d_S4, P->d_psw, st));
+  BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
+                            S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
+                            P->d_S4 + S.n_points, st));
+  Arena A(st);
+  int *d_pi = nullptr, *d_to = nullptr, *d_csr = nullptr, *d_sl = nullptr;
+  double *d_exact = nullptr, *d_approx = nullptr;
+  float* d_err = nullptr;
+  const int n_deg = P->degree - P->degree_min + 1;
+  BTK_TRY(A.upload(&d_pi, std::vector<int>(pair_index, pair_index + n)));
+  BTK_TRY(A.upload(&d_to, std::vector<int>(target_orig, target_orig + (size_t)n * K)));
+  BTK_TRY(A.upload(&d_csr, std::vector<int>(src_leaf_csr, src_leaf_csr + n + 1)));
+  BTK_TRY(A.upload(&d_sl, std::vector<int>(src_leaves, src_leaves + std::max(1, src_leaf_csr[n]))));
+  BTK_TRY(A.alloc(&d_exact, (size_t)n * K * P->ncomp));
+  BTK_TRY(A.alloc(&d_approx, (size_t)n * n_deg * K * P->ncomp));
+  BTK_TRY(A.alloc(&d_err, (size_t)n * n_deg));
+  SampleArgs a{};
+  a.dim = P->dim;
+  a.kind = P->kind;
+  a.ncomp = P->ncomp;
+  a.K = K;
+  a.n_deg = n_deg;
+  a.deg_lo = P->degree_min;
+  a.n = n;
+  a.eps2 = P->eps * P->eps;
+  a.pair_index = d_pi;
+  a.ptype = P->d_pair_type;
+  a.ptgt = P->d_pair_tgt;
+  a.psrc = P->d_pair_src;
+  a.xt = xt;
+  a.yt = yt;
+  a.zt = P->dim == 3 ? zt : nullptr;
+  a.tgt_orig = d_to;
+  a.src_leaf_csr = d_csr;
+  a.src_leaves = d_sl;
+  a.leaf_begin_s = S.d_leaf_begin;
+  a.count_s = S.d_point_count;
+  a.S4 = P->d_S4;
+  a.s_slot_off = P->d_s_slot_off;
+  a.s_slot_begin = P->d_s_cluster_slot_begin;
+  a.cluster_slot_s = P->d_cluster_slot_s;
+  a.T4 = P->d_T4;
+  a.t_slot_off = P->d_t_slot_off;
+  a.t_slot_begin = P->d_t_cluster_slot_begin;
+  a.cluster_slot_t = P->d_cluster_slot_t;
+  a.ns = S.n_points;
+  a.nt = T.n_points;
+  a.pt = T.d_panels;
+  a.slot_d_lo = P->degree_min;
+  a.exact = d_exact;
+  a.approx = d_approx;
+  BTK_CUDA(launch_error_samples(a, d_err, st));
+  BTK_CUDA(cudaMemcpyAsync(log10_err, d_err, sizeof(float) * (size_t)n * n_deg, cudaMemcpyDeviceToHost, st));
+  BTK_CUDA(cudaStreamSynchronize(st));
   return BTK_OK;
 }
 

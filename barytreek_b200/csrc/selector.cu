@@ -1,0 +1,667 @@
+// Learned interpolation-degree selector (no reference counterpart).
+//
+// Per far-field pair (PC, CP, CC) a 16-feature vector describes the geometry
+// (radii, separation ratios, point counts, interaction class, kernel
+// regularisation) and the source cluster's modified charges (Chebyshev-moment
+// band energies from a DCT-I of the degree-n modified charges, net-charge
+// fraction). An MLP 16 -> 64 -> 64 -> 9 with ReLU, BF16 weights and FP32
+// accumulation predicts log10 of the pair's relative far-field error at
+// degrees 4..12; the smallest degree whose prediction meets the pair target is
+// chosen on the device. Training uses error samples generated here: each
+// sampled pair is evaluated at every degree through its proxies and compared
+// with the direct sum over the source cluster's points, in FP64.
+#include "device_math.cuh"
+#include "kernels.cuh"
+
+#include <cuda_bf16.h>
+
+namespace btk {
+
+namespace {
+
+constexpr int kF = 16, kH = 64, kO = 9, kDegLo = 4;
+constexpr int kW1 = 0, kB1 = kW1 + kH * kF, kW2 = kB1 + kH, kB2 = kW2 + kH * kH, kW3 = kB2 + kH, kB3 = kW3 + kO * kH;
+constexpr int kParams = kB3 + kO;  // 5833
+constexpr int kDescs = 6;          // per-panel charge descriptors
+
+__device__ __forceinline__ float lg(double x) { return (float)log10(x > 1e-300 ? x : 1e-300); }
+
+// ---- per-panel charge descriptors ------------------------------------------
+// desc[0] = log10 sum|W|, desc[1] = log10(|sum W| / sum|W|), desc[2..5] =
+// log10 of the Chebyshev-moment energy in bands max(i,j,k) in {1,2}, {3,4},
+// {5,6}, {>=7}, each relative to sum|W|. Moments M = (C x C x C) W with
+// C[i][a] = cos(pi i a / n): Chebyshev moments of the panel's charge
+// distribution (exact through polynomial reproduction).
+__global__ void __launch_bounds__(256) k_panel_desc(int dim, int n, int P, const double* psw, float* desc) {
+  __shared__ double bufA[kMaxNodes * kMaxNodes * kMaxNodes], bufB[kMaxNodes * kMaxNodes * kMaxNodes];
+  __shared__ double C[kMaxNodes * kMaxNodes];
+  __shared__ double red[8][32];
+  const int p = blockIdx.x;
+  const int m = n + 1;
+  const int ipc = dim == 3 ? m * m * m : m * m;
+  const double pi = 3.141592653589793238462643383279502884;
+  for (int o = threadIdx.x; o < m * m; o += blockDim.x) C[o] = cos(pi * (o / m) * (o % m) / n);
+  double l1 = 0.0, s = 0.0;
+  for (int o = threadIdx.x; o < ipc; o += blockDim.x) {
+    const double w = psw[(size_t)p * ipc + o];
+    bufA[o] = w;
+    l1 += fabs(w);
+    s += w;
+  }
+  __syncthreads();
+  // separable DCT-I along each axis (same stride logic as the transfers)
+  const int strides[3] = {dim == 3 ? m * m : m, dim == 3 ? m : 1, 1};
+  double* in = bufA;
+  double* out = bufB;
+  for (int ax = 0; ax < dim; ++ax) {
+    const int str = strides[ax];
+    for (int o = threadIdx.x; o < ipc; o += blockDim.x) {
+      const int i = (o / str) % m;
+      const int base = o - i * str;
+      double acc = 0.0;
+      for (int a = 0; a < m; ++a) acc = fma(C[i * m + a], in[base + a * str], acc);
+      out[o] = acc;
+    }
+    __syncthreads();
+    double* t = in;
+    in = out;
+    out = t;
+  }
+  double band[4] = {0, 0, 0, 0};
+  for (int o = threadIdx.x; o < ipc; o += blockDim.x) {
+    int i, j, k = 0;
+    if (dim == 2) {
+      i = o / m;
+      j = o % m;
+    } else {
+      i = o / (m * m);
+      j = (o / m) % m;
+      k = o % m;
+    }
+    const int mx = max(i, max(j, k));
+    const double e = in[o] * in[o];
+    if (mx >= 1) band[mx <= 2 ? 0 : (mx <= 4 ? 1 : (mx <= 6 ? 2 : 3))] += e;
+  }
+  double v[6] = {l1, s, band[0], band[1], band[2], band[3]};
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int q = 0; q < 6; ++q) {
+    double x = v[q];
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    if (lane == 0) red[wid][q] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[6] = {0, 0, 0, 0, 0, 0};
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w)
+      for (int q = 0; q < 6; ++q) t[q] += red[w][q];
+    const double L1 = t[0] > 1e-300 ? t[0] : 1e-300;
+    float* d = desc + (size_t)p * kDescs;
+    d[0] = lg(L1);
+    d[1] = lg(fabs(t[1]) / L1 + 1e-16);
+    for (int b = 0; b < 4; ++b) d[2 + b] = lg(sqrt(t[2 + b]) / L1 + 1e-16);
+  }
+}
+
+// ---- per-pair features -------------------------------------------------------
+// type: 1 PC, 2 CP, 3 CC. Pairs listed PC, then CP, then CC.
+__global__ void k_pair_features(int n_pairs, const int* ptype, const int* ptgt, const int* psrc,
+                                const DevPanel* pt, const DevPanel* ps, double root_radius, double eps,
+                                const float* desc_s, float* feat) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_pairs) return;
+  const DevPanel T = pt[ptgt[i]], S = ps[psrc[i]];
+  double ct[3], cs[3], rt2 = 0, rs2 = 0, d2 = 0;
+  for (int a = 0; a < 3; ++a) {
+    ct[a] = 0.5 * (T.lo[a] + T.hi[a]);
+    cs[a] = 0.5 * (S.lo[a] + S.hi[a]);
+    rt2 += (T.hi[a] - T.lo[a]) * (T.hi[a] - T.lo[a]);
+    rs2 += (S.hi[a] - S.lo[a]) * (S.hi[a] - S.lo[a]);
+    d2 += (ct[a] - cs[a]) * (ct[a] - cs[a]);
+  }
+  const double rt = 0.5 * sqrt(rt2) + 1e-300, rs = 0.5 * sqrt(rs2) + 1e-300, dist = sqrt(d2) + 1e-300;
+  float* f = feat + (size_t)i * kF;
+  f[0] = lg(rt / root_radius);
+  f[1] = lg(rs / root_radius);
+  f[2] = lg(dist / (rt + rs));
+  f[3] = lg(dist / rs);
+  f[4] = lg(dist / rt);
+  f[5] = lg(1.0 + T.point_count);
+  f[6] = lg(1.0 + S.point_count);
+  f[7] = ptype[i] == 1 ? 1.f : 0.f;
+  f[8] = ptype[i] == 2 ? 1.f : 0.f;
+  f[9] = ptype[i] == 3 ? 1.f : 0.f;
+  f[10] = lg(eps / dist + 1e-12);
+  const float* d = desc_s + (size_t)psrc[i] * kDescs;
+  for (int q = 0; q < 5; ++q) f[11 + q] = d[1 + q];
+}
+
+// ---- MLP ----------------------------------------------------------------------
+// Parameters as BF16, loaded to shared FP32; inputs normalised on the fly.
+struct MlpNorm {
+  float xm[kF], xs[kF], ym, ys;
+};
+
+__device__ __forceinline__ void load_params(const __nv_bfloat16* w, float* sw) {
+  for (int o = threadIdx.x; o < kParams; o += blockDim.x) sw[o] = __bfloat162float(w[o]);
+}
+
+// y[o] for one normalised input row; h1/h2 post-ReLU returned when non-null.
+__device__ __forceinline__ void mlp_row(const float* sw, const float* x, float* y, float* h1o, float* h2o) {
+  float h1[kH], h2[kH];
+#pragma unroll 4
+  for (int j = 0; j < kH; ++j) {
+    float a = sw[kB1 + j];
+#pragma unroll
+    for (int i = 0; i < kF; ++i) a = fmaf(sw[kW1 + j * kF + i], x[i], a);
+    h1[j] = fmaxf(a, 0.f);
+  }
+#pragma unroll 2
+  for (int j = 0; j < kH; ++j) {
+    float a = sw[kB2 + j];
+#pragma unroll 8
+    for (int i = 0; i < kH; ++i) a = fmaf(sw[kW2 + j * kH + i], h1[i], a);
+    h2[j] = fmaxf(a, 0.f);
+  }
+#pragma unroll
+  for (int o = 0; o < kO; ++o) {
+    float a = sw[kB3 + o];
+#pragma unroll 8
+    for (int i = 0; i < kH; ++i) a = fmaf(sw[kW3 + o * kH + i], h2[i], a);
+    y[o] = a;
+  }
+  if (h1o)
+    for (int j = 0; j < kH; ++j) h1o[j] = h1[j];
+  if (h2o)
+    for (int j = 0; j < kH; ++j) h2o[j] = h2[j];
+}
+
+// Inference on raw features: out[i][o] = predicted log10 error at degree 4+o.
+__global__ void __launch_bounds__(128) k_mlp_infer(int n, const __nv_bfloat16* w, MlpNorm nrm, const float* feat,
+                                                   float* out) {
+  extern __shared__ float sw[];
+  load_params(w, sw);
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float x[kF], y[kO];
+  for (int k = 0; k < kF; ++k) x[k] = (feat[(size_t)i * kF + k] - nrm.xm[k]) / nrm.xs[k];
+  mlp_row(sw, x, y, nullptr, nullptr);
+  for (int o = 0; o < kO; ++o) out[(size_t)i * kO + o] = y[o] * nrm.ys + nrm.ym;
+}
+
+// Forward on normalised inputs (training/validation): yn[i][o].
+__global__ void __launch_bounds__(128) k_mlp_forward_n(int n, const __nv_bfloat16* w, const float* xn, float* yn) {
+  extern __shared__ float sw[];
+  load_params(w, sw);
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float y[kO];
+  mlp_row(sw, xn + (size_t)i * kF, y, nullptr, nullptr);
+  for (int o = 0; o < kO; ++o) yn[(size_t)i * kO + o] = y[o];
+}
+
+// Per-sample forward + backward of the masked mean-squared error
+// L = sum_{i,o} mask (y - t)^2 / sum mask. Stores post-ReLU activations and
+// pre-activation deltas for the weight-gradient reduction.
+__global__ void __launch_bounds__(128) k_mlp_backprop(int n, const __nv_bfloat16* w, const float* xn, const float* tn,
+                                                      const float* mask, float inv_count, float* h1s, float* h2s,
+                                                      float* d1s, float* d2s, float* d3s, float* loss) {
+  extern __shared__ float sw[];
+  load_params(w, sw);
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float lsum = 0.f;
+  if (i < n) {
+    float y[kO], h1[kH], h2[kH], d3[kO], d2[kH];
+    mlp_row(sw, xn + (size_t)i * kF, y, h1, h2);
+    for (int o = 0; o < kO; ++o) {
+      const float mk = mask[(size_t)i * kO + o];
+      const float e = y[o] - tn[(size_t)i * kO + o];
+      lsum += mk * e * e;
+      d3[o] = 2.f * mk * e * inv_count;
+      d3s[(size_t)i * kO + o] = d3[o];
+    }
+    for (int j = 0; j < kH; ++j) {
+      float a = 0.f;
+      for (int o = 0; o < kO; ++o) a = fmaf(sw[kW3 + o * kH + j], d3[o], a);
+      d2[j] = h2[j] > 0.f ? a : 0.f;
+      d2s[(size_t)i * kH + j] = d2[j];
+      h1s[(size_t)i * kH + j] = h1[j];
+      h2s[(size_t)i * kH + j] = h2[j];
+    }
+    for (int j = 0; j < kH; ++j) {
+      float a = 0.f;
+      for (int k = 0; k < kH; ++k) a = fmaf(sw[kW2 + k * kH + j], d2[k], a);
+      d1s[(size_t)i * kH + j] = h1[j] > 0.f ? a : 0.f;
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, off);
+  if ((threadIdx.x & 31) == 0 && lsum != 0.f) atomicAdd(loss, lsum * inv_count);
+}
+
+// Weight gradients: one thread per parameter, summing over the batch.
+__global__ void k_mlp_wgrad(int n, const float* xn, const float* h1s, const float* h2s, const float* d1s,
+                            const float* d2s, const float* d3s, float* grad) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kParams) return;
+  float g = 0.f;
+  if (p < kB1) {
+    const int j = p / kF, k = p % kF;
+    for (int i = 0; i < n; ++i) g = fmaf(d1s[(size_t)i * kH + j], xn[(size_t)i * kF + k], g);
+  } else if (p < kW2) {
+    const int j = p - kB1;
+    for (int i = 0; i < n; ++i) g += d1s[(size_t)i * kH + j];
+  } else if (p < kB2) {
+    const int j = (p - kW2) / kH, k = (p - kW2) % kH;
+    for (int i = 0; i < n; ++i) g = fmaf(d2s[(size_t)i * kH + j], h1s[(size_t)i * kH + k], g);
+  } else if (p < kW3) {
+    const int j = p - kB2;
+    for (int i = 0; i < n; ++i) g += d2s[(size_t)i * kH + j];
+  } else if (p < kB3) {
+    const int o = (p - kW3) / kH, k = (p - kW3) % kH;
+    for (int i = 0; i < n; ++i) g = fmaf(d3s[(size_t)i * kO + o], h2s[(size_t)i * kH + k], g);
+  } else {
+    const int o = p - kB3;
+    for (int i = 0; i < n; ++i) g += d3s[(size_t)i * kO + o];
+  }
+  grad[p] = g;
+}
+
+// Adam on FP32 master weights; the BF16 copy is what the network runs with.
+__global__ void k_adam(float* master, __nv_bfloat16* w, const float* grad, float* m, float* v, float lr, float b1,
+                       float b2, float eps, float c1, float c2) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kParams) return;
+  const float g = grad[p];
+  const float mm = b1 * m[p] + (1.f - b1) * g;
+  const float vv = b2 * v[p] + (1.f - b2) * g * g;
+  m[p] = mm;
+  v[p] = vv;
+  const float upd = lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+  master[p] -= upd;
+  w[p] = __float2bfloat16_rn(master[p]);
+}
+
+// Degree choice: the smallest d in [lo, hi] with prediction <= target, else hi.
+__global__ void k_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int* deg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int d = hi;
+  for (int c = max(lo, kDegLo); c <= hi && c < kDegLo + kO; ++c)
+    if (pred[(size_t)i * kO + (c - kDegLo)] <= log10_target) {
+      d = c;
+      break;
+    }
+  deg[i] = d;
+}
+
+// Far-field evaluations at the chosen degrees (pairs PC, CP, CC in order).
+__global__ void k_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
+                            const int* cp_scount, unsigned long long* evals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long v = 0;
+  const int n = n_pc + n_cp + n_cc;
+  if (i < n) {
+    const unsigned long long m = (unsigned long long)(deg[i] + 1);
+    const unsigned long long s = dim == 3 ? m * m * m : m * m;
+    if (i < n_pc)
+      v = s * (unsigned long long)pc_tcount[i];
+    else if (i < n_pc + n_cp)
+      v = s * (unsigned long long)cp_scount[i - n_pc];
+    else
+      v = s * s;
+  }
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(evals, v);
+}
+
+// Audit: sums of |treecode - direct|^2 and |direct|^2 over the audited
+// targets and all components.
+__global__ void k_audit_compare(int n, int ncomp, int nt, const int* audit_sorted, const int* perm, const double* out,
+                                const double* audit_out, double* sums) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0, r = 0.0;
+  if (i < n) {
+    const int orig = perm ? perm[audit_sorted[i]] : audit_sorted[i];
+    for (int c = 0; c < ncomp; ++c) {
+      const double a = out[(size_t)c * nt + orig], b = audit_out[(size_t)c * n + i];
+      e += (a - b) * (a - b);
+      r += b * b;
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    e += __shfl_down_sync(0xffffffffu, e, off);
+    r += __shfl_down_sync(0xffffffffu, r, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(sums, e);
+    atomicAdd(sums + 1, r);
+  }
+}
+
+// ---- training samples ----------------------------------------------------------
+// Kernel value with its constant, FP64, into acc[c] (c < ncomp).
+template <int DIM>
+__device__ __forceinline__ void kval(int kind, double eps2, const double* t, const double4& s, double* acc) {
+  const double dx = t[0] - s.x, dy = t[1] - s.y, dz = DIM == 3 ? t[2] - s.z : 0.0;
+  const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+  const double pi = 3.141592653589793238462643383279502884;
+  if (DIM == 2) {
+    acc[0] += s.w * log(r2) / (4.0 * pi);
+    if (kind == BTK_KIND_FIELD) {
+      const double g = -s.w / (2.0 * pi * r2);
+      acc[1] += dx * g;
+      acc[2] += dy * g;
+    }
+    return;
+  }
+  if (kind == BTK_KIND_VEL) {
+    const double g = -s.w / (4.0 * pi * r2);
+    acc[0] += dx * g;
+    acc[1] += dy * g;
+    acc[2] += dz * g;
+    return;
+  }
+  const double ri = 1.0 / sqrt(r2);
+  acc[0] += -s.w * ri / (4.0 * pi);
+  if (kind == BTK_KIND_FIELD) {
+    const double g = -s.w * ri * ri * ri / (4.0 * pi);
+    acc[1] += dx * g;
+    acc[2] += dy * g;
+    acc[3] += dz * g;
+  }
+}
+
+
+
+__device__ __forceinline__ void target_point(const SampleArgs& a, int s, int k, double* t) {
+  const int i = a.tgt_orig[(size_t)s * a.K + k];
+  t[0] = a.xt[i];
+  t[1] = a.yt[i];
+  t[2] = a.dim == 3 ? a.zt[i] : 0.0;
+}
+
+// One block per sample: direct sum over every point under the source panel.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_sample_exact(SampleArgs a) {
+  __shared__ double red[256][4];
+  const int s = blockIdx.x;
+  const int lanes = blockDim.x / a.K;  // threads per target
+  const int k = threadIdx.x / lanes, part = threadIdx.x % lanes;
+  double acc[4] = {0, 0, 0, 0};
+  if (k < a.K) {
+    double t[3];
+    target_point(a, s, k, t);
+    for (int l = a.src_leaf_csr[s]; l < a.src_leaf_csr[s + 1]; ++l) {
+      const int leaf = a.src_leaves[l];
+      const int b = a.leaf_begin_s[leaf], c = a.count_s[leaf];
+      for (int j = part; j < c; j += lanes) kval<DIM>(a.kind, a.eps2, t, a.S4[b + j], acc);
+    }
+  }
+  for (int c = 0; c < 4; ++c) red[threadIdx.x][c] = acc[c];
+  __syncthreads();
+  if (k < a.K && part == 0) {
+    for (int c = 0; c < a.ncomp; ++c) {
+      double v = 0.0;
+      for (int q = 0; q < lanes; ++q) v += red[threadIdx.x + q][c];
+      a.exact[((size_t)s * a.K + k) * a.ncomp + c] = v;
+    }
+  }
+}
+
+// One block per (sample, degree): the pair's contribution at the sample's
+// targets through its degree-d proxies.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_sample_approx(SampleArgs a) {
+  extern __shared__ double phi[];  // [ncomp][(d+1)^DIM]
+  __shared__ double red[256][4];
+  const int s = blockIdx.x / a.n_deg, di = blockIdx.x % a.n_deg;
+  const int d = a.deg_lo + di, md = d + 1;
+  const int ipc = DIM == 3 ? md * md * md : md * md;
+  const int p = a.pair_index[s];
+  const int type = a.ptype[p];
+  const int tgt = a.ptgt[p], src = a.psrc[p];
+  double* outp = a.approx + ((size_t)s * a.n_deg + di) * a.K * a.ncomp;
+  // source slot of degree d (PC, CC) or the source leaf (CP)
+  long long sb = 0;
+  int sc = 0;
+  if (type == 2) {
+    sb = a.leaf_begin_s[src];
+    sc = a.count_s[src];
+  } else {
+    const int slot = a.s_slot_begin[a.cluster_slot_s[src]] + (d - a.slot_d_lo);
+    sb = a.ns + a.s_slot_off[slot];
+    sc = ipc;
+  }
+  if (type == 1) {  // PC: targets against the degree-d source proxies
+    const int lanes = blockDim.x / a.K;
+    const int k = threadIdx.x / lanes, part = threadIdx.x % lanes;
+    double acc[4] = {0, 0, 0, 0};
+    if (k < a.K) {
+      double t[3];
+      target_point(a, s, k, t);
+      for (int j = part; j < sc; j += lanes) kval<DIM>(a.kind, a.eps2, t, a.S4[sb + j], acc);
+    }
+    for (int c = 0; c < 4; ++c) red[threadIdx.x][c] = acc[c];
+    __syncthreads();
+    if (k < a.K && part == 0)
+      for (int c = 0; c < a.ncomp; ++c) {
+        double v = 0.0;
+        for (int q = 0; q < lanes; ++q) v += red[threadIdx.x + q][c];
+        outp[(size_t)k * a.ncomp + c] = v;
+      }
+    return;
+  }
+  // CP, CC: potentials at the target's degree-d proxies, then interpolation.
+  const int tslot = a.t_slot_begin[a.cluster_slot_t[tgt]] + (d - a.slot_d_lo);
+  const double4* tp = a.T4 + a.nt + a.t_slot_off[tslot];
+  for (int j = threadIdx.x; j < ipc; j += blockDim.x) {
+    const double4 tq = tp[j];
+    const double t[3] = {tq.x, tq.y, tq.z};
+    double acc[4] = {0, 0, 0, 0};
+    for (int q = 0; q < sc; ++q) kval<DIM>(a.kind, a.eps2, t, a.S4[sb + q], acc);
+    for (int c = 0; c < a.ncomp; ++c) phi[(size_t)c * ipc + j] = acc[c];
+  }
+  __syncthreads();
+  const DevPanel T = a.pt[tgt];
+  const double pi = 3.141592653589793238462643383279502884;
+  for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
+    double t[3];
+    target_point(a, s, k, t);
+    double L[3][kMaxNodes];
+    for (int ax = 0; ax < DIM; ++ax) {
+      const double range = 0.5 * (T.hi[ax] - T.lo[ax]), mid = 0.5 * (T.hi[ax] + T.lo[ax]);
+      int hit = -1;
+      double den = 0.0;
+      for (int i = 0; i < md; ++i) {
+        const double node = cos(pi * i / d) * range + mid;
+        const double diff = t[ax] - node;
+        if (hit < 0 && fabs(diff) < 2.220446049250313e-16) hit = i;
+        const double w = ((i & 1) ? -1.0 : 1.0) * ((i == 0 || i == d) ? 0.5 : 1.0);
+        L[ax][i] = w / diff;
+        den += L[ax][i];
+      }
+      for (int i = 0; i < md; ++i) L[ax][i] = hit >= 0 ? (i == hit ? 1.0 : 0.0) : L[ax][i] / den;
+    }
+    for (int c = 0; c < a.ncomp; ++c) {
+      double v = 0.0;
+      for (int j = 0; j < ipc; ++j) {
+        const int i0 = DIM == 3 ? j / (md * md) : j / md, i1 = DIM == 3 ? (j / md) % md : j % md;
+        double b = L[0][i0] * L[1][i1];
+        if (DIM == 3) b *= L[2][j % md];
+        v += phi[(size_t)c * ipc + j] * b;
+      }
+      outp[(size_t)k * a.ncomp + c] = v;
+    }
+  }
+}
+
+// log10 of the relative L2 error of each degree against the exact values.
+__global__ void k_sample_errors(int n, int n_deg, int K, int ncomp, const double* exact, const double* approx,
+                                float* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * n_deg) return;
+  const int s = i / n_deg, di = i % n_deg;
+  double e = 0.0, r = 0.0;
+  for (int q = 0; q < K * ncomp; ++q) {
+    const double x = exact[(size_t)s * K * ncomp + q];
+    const double y = approx[((size_t)s * n_deg + di) * K * ncomp + q];
+    e += (x - y) * (x - y);
+    r += x * x;
+  }
+  out[i] = (float)log10(sqrt(e / (r > 1e-300 ? r : 1e-300)) + 1e-30);
+}
+
+__global__ void k_fill_int(int n, int value, int* dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = value;
+}
+
+}  // namespace
+
+// ---- launchers -----------------------------------------------------------------
+int selector_param_count() { return kParams; }
+
+cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
+                             const int* cp_scount, unsigned long long* evals, cudaStream_t s) {
+  const int n = n_pc + n_cp + n_cc;
+  if (n <= 0) return cudaSuccess;
+  k_far_evals<<<(n + 255) / 256, 256, 0, s>>>(dim, n_pc, n_cp, n_cc, deg, pc_tcount, cp_scount, evals);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_audit_compare(int n, int ncomp, int nt, const int* audit_sorted, const int* perm,
+                                 const double* out, const double* audit_out, double* sums, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_audit_compare<<<(n + 255) / 256, 256, 0, s>>>(n, ncomp, nt, audit_sorted, perm, out, audit_out, sums);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_error_samples(const SampleArgs& a, float* log10_err, cudaStream_t s) {
+  if (a.n <= 0) return cudaSuccess;
+  const int md = a.deg_lo + a.n_deg;  // highest degree + 1
+  const size_t shm = sizeof(double) * a.ncomp * (a.dim == 3 ? md * md * md : md * md);
+  if (a.dim == 2) {
+    k_sample_exact<2><<<a.n, 256, 0, s>>>(a);
+    cudaFuncSetAttribute(k_sample_approx<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    k_sample_approx<2><<<a.n * a.n_deg, 256, shm, s>>>(a);
+  } else {
+    k_sample_exact<3><<<a.n, 256, 0, s>>>(a);
+    cudaFuncSetAttribute(k_sample_approx<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    k_sample_approx<3><<<a.n * a.n_deg, 256, shm, s>>>(a);
+  }
+  const int m = a.n * a.n_deg;
+  k_sample_errors<<<(m + 255) / 256, 256, 0, s>>>(a.n, a.n_deg, a.K, a.ncomp, a.exact, a.approx, log10_err);
+  count_launch(3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_int(int n, int value, int* dst, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_fill_int<<<(n + 255) / 256, 256, 0, s>>>(n, value, dst);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_panel_desc(int dim, int n, int P, const double* psw, float* desc, cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  k_panel_desc<<<P, 256, 0, s>>>(dim, n, P, psw, desc);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_features(int n_pairs, const int* ptype, const int* ptgt, const int* psrc, const DevPanel* pt,
+                                 const DevPanel* ps, double root_radius, double eps, const float* desc_s, float* feat,
+                                 cudaStream_t s) {
+  if (n_pairs <= 0) return cudaSuccess;
+  k_pair_features<<<(n_pairs + 127) / 128, 128, 0, s>>>(n_pairs, ptype, ptgt, psrc, pt, ps, root_radius, eps, desc_s,
+                                                        feat);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const float* feat, float* out,
+                             cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  MlpNorm nrm;
+  for (int k = 0; k < kF; ++k) {
+    nrm.xm[k] = norm[k];
+    nrm.xs[k] = norm[kF + k] > 0 ? norm[kF + k] : 1.f;
+  }
+  nrm.ym = norm[2 * kF];
+  nrm.ys = norm[2 * kF + 1] > 0 ? norm[2 * kF + 1] : 1.f;
+  const size_t shm = sizeof(float) * kParams;
+  cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  k_mlp_infer<<<(n + 127) / 128, 128, shm, s>>>(n, (const __nv_bfloat16*)w_bf16, nrm, feat, out);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int* deg,
+                                  cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_choose_degrees<<<(n + 255) / 256, 256, 0, s>>>(n, pred, log10_target, lo, hi, deg);
+  count_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace btk
+
+using namespace btk;
+
+extern "C" {
+
+int btk_selector_param_count(void) { return kParams; }
+
+btk_status btk_mlp_forward(const void* w_bf16, int n, const float* xn, float* yn, btk_stream_t stream) {
+  BTK_CHECK(w_bf16 && n >= 0 && (n == 0 || (xn && yn)), BTK_ERR_INVALID_ARGUMENT, "btk_mlp_forward: bad argument");
+  if (n == 0) return BTK_OK;
+  const size_t shm = sizeof(float) * kParams;
+  BTK_CUDA(cudaFuncSetAttribute(k_mlp_forward_n, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+  k_mlp_forward_n<<<(n + 127) / 128, 128, shm, (cudaStream_t)stream>>>(n, (const __nv_bfloat16*)w_bf16, xn, yn);
+  count_launch();
+  BTK_CUDA(cudaGetLastError());
+  return BTK_OK;
+}
+
+btk_status btk_mlp_gradient(const void* w_bf16, int n, const float* xn, const float* tn, const float* mask,
+                            float* grad, float* loss, float* work, btk_stream_t stream) {
+  BTK_CHECK(w_bf16 && n > 0 && xn && tn && mask && grad && loss && work, BTK_ERR_INVALID_ARGUMENT,
+            "btk_mlp_gradient: bad argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  float* h1 = work;
+  float* h2 = h1 + (size_t)n * kH;
+  float* d1 = h2 + (size_t)n * kH;
+  float* d2 = d1 + (size_t)n * kH;
+  float* d3 = d2 + (size_t)n * kH;
+  // normalisation of the loss: the number of unmasked targets is taken as
+  // n * outputs (masked entries contribute zero).
+  const float inv = 1.f / (float)((size_t)n * kO);
+  BTK_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), st));
+  const size_t shm = sizeof(float) * kParams;
+  BTK_CUDA(cudaFuncSetAttribute(k_mlp_backprop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+  k_mlp_backprop<<<(n + 127) / 128, 128, shm, st>>>(n, (const __nv_bfloat16*)w_bf16, xn, tn, mask, inv, h1, h2, d1,
+                                                    d2, d3, loss);
+  count_launch();
+  k_mlp_wgrad<<<(kParams + 127) / 128, 128, 0, st>>>(n, xn, h1, h2, d1, d2, d3, grad);
+  count_launch();
+  BTK_CUDA(cudaGetLastError());
+  return BTK_OK;
+}
+
+btk_status btk_mlp_adam(float* master, void* w_bf16, const float* grad, float* m, float* v, int step, float lr,
+                        btk_stream_t stream) {
+  BTK_CHECK(master && w_bf16 && grad && m && v && step >= 1, BTK_ERR_INVALID_ARGUMENT, "btk_mlp_adam: bad argument");
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  k_adam<<<(kParams + 127) / 128, 128, 0, (cudaStream_t)stream>>>(master, (__nv_bfloat16*)w_bf16, grad, m, v, lr, b1,
+                                                                  b2, 1e-8f, c1, c2);
+  count_launch();
+  BTK_CUDA(cudaGetLastError());
+  return BTK_OK;
+}
+
+}  // extern "C"

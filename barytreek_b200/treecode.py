@@ -218,6 +218,28 @@ class Treecode:
                                       ptr(out), stream))
         return out
 
+    def solve_learned(self, charges, selector, tol=1e-6, pair_tol=None, degree_lo=4, out=None):
+        """Learned-degree solve with a 1% direct-sum audit and fallback
+        (btk_plan_execute_learned). Returns (out tensor, report dict)."""
+        import torch
+
+        q = charges if isinstance(charges, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(charges, np.float64))
+        q = q.to(self.device, torch.float64).contiguous()
+        if out is None:
+            out = torch.empty((self.ncomp, self.nt), dtype=torch.float64, device=self.device)
+        pair_tol = tol * 0.2 if pair_tol is None else pair_tol
+        t, s = self._t, self._s
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        z_t = ptr(t[2]) if self.dim == 3 else None
+        z_s = ptr(s[2]) if self.dim == 3 else None
+        rep = _lib.LearnedReport()
+        check(load().btk_plan_execute_learned(self._plan, selector.handle(), tol, pair_tol, degree_lo, ptr(t[0]),
+                                              ptr(t[1]), z_t, ptr(s[0]), ptr(s[1]), z_s, ptr(q), ptr(out),
+                                              ctypes.byref(rep), stream))
+        r = {k: getattr(rep, k) for k, _ in rep._fields_ if k != "degree_hist"}
+        r["degree_hist"] = list(rep.degree_hist)
+        return out, r
+
     def last_timing(self) -> dict:
         ms = (ctypes.c_float * 5)()
         check(load().btk_plan_last_timing(self._plan, ms))

@@ -319,6 +319,78 @@ btk_status btk_solve_host(int dim, int kind, int precision, int degree, int clus
                           double eps, int n, const double* x, const double* y, const double* z,
                           const double* charges, double* out, btk_stream_t stream);
 
+/* ---- Learned degree selector (no reference counterpart) ------------------
+ *
+ * An MLP 16 -> 64 -> 64 -> 9 (ReLU) with BF16 weights and FP32 accumulation
+ * predicts, for every far-field pair (PC, CP, CC) of a BTK_DEGREE_PER_PAIR
+ * plan, log10 of the pair's relative error at degrees 4..12 from 16 features
+ * (geometry ratios, point counts, class, eps/distance, Chebyshev-moment band
+ * energies of the source's modified charges). Parameter layout (FP32, 5833):
+ * W1[64][16], b1[64], W2[64][64], b2[64], W3[9][64], b3[9]. norm[34]: feature
+ * means[16], feature std[16], target mean, target std (the network sees
+ * normalised inputs and predicts normalised targets). */
+typedef struct btk_selector btk_selector;
+int btk_selector_param_count(void);
+btk_status btk_selector_create(btk_selector** sel, const float* params, const float* norm);
+btk_status btk_selector_destroy(btk_selector* sel);
+const void* btk_selector_weights(const btk_selector* sel); /* device BF16 parameters */
+
+/* Far-field pairs of a per-pair plan (PC, then CP, then CC, list order). */
+btk_status btk_plan_pair_count(const btk_plan* plan, int* n_pairs);
+/* Runs the upward pass for these sources/charges and writes the features of
+ * every far-field pair: device float features[n_pairs][16]. */
+btk_status btk_plan_pair_features(btk_plan* plan, const double* xs, const double* ys, const double* zs,
+                                  const double* charges, float* features, btk_stream_t stream);
+
+typedef struct {
+  double audit_rel_l2; /* treecode vs direct sum over the audited targets */
+  int audit_targets;   /* 1% of the targets (fixed, seeded sample) */
+  int fell_back;       /* 1: audit above tol, the fixed-degree FP64 result was returned */
+  int64_t evals_near;  /* PP evaluations */
+  int64_t evals_far;   /* PC + CP + CC evaluations at the chosen degrees */
+  float ms_select;     /* upward pass + features + network + degree choice */
+  float ms_solve;      /* interactions + promotion + downward at the chosen degrees */
+  float ms_total;      /* everything, audit and fallback included */
+  int degree_hist[13]; /* far-field pairs per chosen degree */
+} btk_learned_report;
+
+/* Learned-degree solve: upward pass, features, network, per-pair degree =
+ * the smallest d in [max(degree_lo, degree_min), interp_degree] whose
+ * predicted error is <= pair_tol, interactions at those degrees (the plan's
+ * precision), downward pass; then a direct-sum audit of 1% of the targets.
+ * When the audit's relative L2 exceeds tol, the fixed-degree FP64 result is
+ * computed and returned instead (report->fell_back = 1). Synchronises the
+ * stream once (to read the audit). out as btk_plan_execute. */
+btk_status btk_plan_execute_learned(btk_plan* plan, const btk_selector* sel, double tol, double pair_tol,
+                                    int degree_lo, const double* xt, const double* yt, const double* zt,
+                                    const double* xs, const double* ys, const double* zs, const double* charges,
+                                    double* out, btk_learned_report* report, btk_stream_t stream);
+
+/* Training samples, generated by the treecode itself: for n sampled far-field
+ * pairs (pair_index into the plan's pair list), the relative L2 error of the
+ * pair's contribution at K target points (target_orig: original indices,
+ * [n][K]) computed through the pair's degree-d proxies, for every degree
+ * d = degree_min..interp_degree, against the FP64 direct sum over the points
+ * under the pair's source panel (src_leaf_csr[n+1] / src_leaves: the leaf
+ * panels under each source). Coordinates and charges are device arrays as in
+ * btk_plan_execute. log10_err: host float [n][interp_degree - degree_min + 1]. */
+btk_status btk_plan_error_samples(btk_plan* plan, const double* xt, const double* yt, const double* zt,
+                                  const double* xs, const double* ys, const double* zs, const double* charges, int n,
+                                  const int* pair_index, int K, const int* target_orig, const int* src_leaf_csr,
+                                  const int* src_leaves, float* log10_err, btk_stream_t stream);
+
+/* Training kernels (device arrays). Inputs xn are normalised features
+ * [n][16], targets tn normalised [n][9], mask [n][9] (0/1). */
+btk_status btk_mlp_forward(const void* w_bf16, int n, const float* xn, float* yn, btk_stream_t stream);
+/* Masked mean-squared error L = sum mask (y - t)^2 / (9 n) and dL/dparams
+ * (FP32, 5833 entries). work: 4*64*n + 9*n floats. */
+btk_status btk_mlp_gradient(const void* w_bf16, int n, const float* xn, const float* tn, const float* mask,
+                            float* grad, float* loss, float* work, btk_stream_t stream);
+/* One Adam step (beta 0.9/0.999) on FP32 master parameters; refreshes the
+ * BF16 copy the network runs with. step counts from 1. */
+btk_status btk_mlp_adam(float* master, void* w_bf16, const float* grad, float* m, float* v, int step, float lr,
+                        btk_stream_t stream);
+
 /* Sustained fused-multiply-add rate of this GPU's FP64 (which = 0) or FP32
  * (which = 1) CUDA-core pipe, in TFLOP/s (2 flops per FMA), measured by a
  * probe kernel with independent FMA chains on every SM. The roofline
