@@ -86,14 +86,58 @@ def _per_pair_tree(seed=3, n=6000, deg=8, leaf=150):
     return tc, pts, q
 
 
-def test_error_samples_match_oracle(oracle):
-    from barytreek_b200 import selector
-    tc, pts, q = _per_pair_tree()
-    feat, errs = selector.generate_samples(tc, q, n_samples=6, K=16, seed=5)
-    assert feat.shape == (6, 16) and errs.shape == (6, 5)
-    # errors decrease with degree (typically) and are finite
-    assert np.all(np.isfinite(errs))
-    assert np.mean(errs[:, 0] > errs[:, -1]) >= 0.8
+def test_error_samples_match_oracle(oracle, lib):
+    import torch
+    from barytreek_b200 import _lib, selector
+    tc, pts, q = _per_pair_tree(n=4000, deg=7, leaf=100)
+    pp, pc, cp, cc = tc.lists
+    lists = [("pc", pc), ("cp", cp), ("cc", cc)]
+    rng = np.random.default_rng(9)
+    K = 8
+    picks = []  # (pair index in the PC,CP,CC order, class name, pair)
+    off = 0
+    for name, l in lists:
+        for i in rng.choice(len(l), size=min(2, len(l)), replace=False):
+            picks.append((off + int(i), name, l[i]))
+        off += len(l)
+    P = tc.tree_t.panels
+    tgt_orig, csr, leaves = [], [0], []
+    for _, _, pr in picks:
+        lv = selector._subtree_leaves(P, int(pr["target_panel"]))
+        pts_t = np.concatenate([tc.tree_t.panel_points_inside[l, :P["point_count"][l]] for l in lv])
+        tgt_orig.append(pts_t[rng.integers(0, len(pts_t), K)])
+        sl = selector._subtree_leaves(P, int(pr["source_panel"]))
+        leaves += sl
+        csr.append(len(leaves))
+    tgt_orig = np.ascontiguousarray(np.array(tgt_orig), np.int32)
+    csr, leaves = np.asarray(csr, np.int32), np.asarray(leaves, np.int32)
+    pidx = np.asarray([p[0] for p in picks], np.int32)
+    n_deg = 7 - 4 + 1
+    out = np.zeros((len(picks), n_deg), np.float32)
+    Q = torch.from_numpy(q).cuda()
+    t, s = tc._t, tc._s
+    _lib.check(lib.btk_plan_error_samples(tc._plan, _lib.ptr(t[0]), _lib.ptr(t[1]), _lib.ptr(t[2]), _lib.ptr(s[0]),
+                                          _lib.ptr(s[1]), _lib.ptr(s[2]), _lib.ptr(Q), len(picks), _lib.ptr(pidx), K,
+                                          _lib.ptr(tgt_orig), _lib.ptr(csr), _lib.ptr(leaves), _lib.ptr(out), None))
+    base = {"dim": 3, "degree": 7, "eps": 1e-4, "thresh": 100, "targets": pts, "sources": pts, "panels_t": P,
+            "panels_s": P, "level_start_t": tc.tree_t.level_start, "level_start_s": tc.tree_t.level_start,
+            "leaf_of_s": tc.tree_t.point_leaf_panel, "inside_t": tc.tree_t.panel_points_inside,
+            "inside_s": tc.tree_t.panel_points_inside}
+    empty = np.zeros(0, pc.dtype)
+    for j, (_, name, pr) in enumerate(picks):
+        src_pts = np.concatenate([tc.tree_t.panel_points_inside[l, :P["point_count"][l]]
+                                  for l in leaves[csr[j]:csr[j + 1]]])
+        mask = np.zeros(len(q))
+        mask[src_pts] = 1.0
+        tg = tuple(c[tgt_orig[j]] for c in pts)
+        exact = oracle.direct(3, 2, 1e-4, tg, pts, q * mask)
+        for di, d in enumerate(range(4, 8)):
+            tree = dict(base, pp=empty, pc=empty, cp=empty, cc=empty)
+            tree[name] = np.array([pr], pc.dtype)
+            approx = oracle.solve_degrees(tree, 2, q, np.full(1, d), np.full(1, d), np.full(1, d))[:, tgt_orig[j]]
+            e_ref = np.log10(np.linalg.norm(approx - exact) / np.linalg.norm(exact) + 1e-30)
+            if e_ref > -11:
+                assert abs(out[j, di] - e_ref) <= 0.05, (name, d, out[j, di], e_ref)
 
 
 def test_learned_solve_audit_gain_and_fallback(oracle):
