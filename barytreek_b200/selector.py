@@ -112,7 +112,11 @@ def generate_samples(tc, charges, n_samples: int, K: int = 32, seed: int = 0, ba
     tg = np.concatenate([pc["target_panel"], cp["target_panel"], cc["target_panel"]])
     sr = np.concatenate([pc["source_panel"], cp["source_panel"], cc["source_panel"]])
     tt, st = tc.tree_t, (tc.tree_s or tc.tree_t)
-    pick = rng.choice(n_pairs, size=min(n_samples, n_pairs), replace=n_samples > n_pairs)
+    # empty leaves appear in the lists; their pairs carry no signal
+    valid = np.flatnonzero((tt.panels["point_count"][tg] > 0) & (st.panels["point_count"][sr] > 0))
+    if len(valid) == 0:
+        return np.zeros((0, N_FEATURES), np.float32), np.zeros((0, 0), np.float32)
+    pick = valid[rng.choice(len(valid), size=min(n_samples, len(valid)), replace=n_samples > len(valid))]
     n_deg = tc.cfg.interp_degree - tc.degree_min + 1
     errs = np.zeros((len(pick), n_deg), np.float32)
     leaves_cache_t, leaves_cache_s = {}, {}

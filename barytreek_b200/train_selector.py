@@ -1,0 +1,89 @@
+"""Trains the learned degree selector on the GPU and writes a weight file.
+
+    python -m barytreek_b200.train_selector --out barytreek_b200/selector_weights.npz
+
+Error samples come from a family of synthetic 3-D problems (Plummer spheres,
+uniform cubes, sphere surfaces, Gaussian mixtures; several seeds, sizes, leaf
+sizes and MAC parameters) solved by BTK_DEGREE_PER_PAIR plans of degree 12, so
+every network output (degrees 4..12) is observed. The network is trained with
+the library's BF16 forward/backward kernels and Adam (barytreek_b200.selector).
+Samples are cached in an .npz next to the output so training can resume.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import time
+
+import numpy as np
+
+from . import datagen, selector
+from .treecode import Treecode, KIND_FIELD
+from ._lib import DEGREE_PER_PAIR
+
+# (family, N, leaf, theta, eps, seed)
+FAMILY = [
+    ("plummer", 1 << 19, 2000, 0.7, 1e-4, 101),
+    ("plummer", 1 << 18, 1000, 0.6, 1e-4, 102),
+    ("plummer", 1 << 19, 1500, 0.8, 1e-3, 103),
+    ("uniform", 1 << 19, 2000, 0.7, 1e-4, 104),
+    ("uniform", 1 << 18, 800, 0.6, 1e-4, 105),
+    ("sphere", 1 << 19, 2000, 0.8, 1e-3, 106),
+    ("sphere", 1 << 18, 1000, 0.7, 1e-4, 107),
+    ("mixture", 1 << 19, 1500, 0.6, 1e-4, 108),
+    ("mixture", 1 << 18, 600, 0.7, 1e-4, 109),
+]
+
+
+def problem(family, n, seed):
+    if family == "plummer":
+        return datagen.plummer(seed, n)
+    if family == "uniform":
+        return datagen.uniform_box(seed, n, 3, 0.0, 1.0)
+    if family == "sphere":
+        return datagen.sphere_surface(seed, n)
+    return datagen.gaussian_mixture(seed, n)
+
+
+def collect(n_total, K=16, log=print):
+    per = max(1, n_total // len(FAMILY))
+    Xs, Es = [], []
+    for fam, n, leaf, theta, eps, seed in FAMILY:
+        t0 = time.time()
+        pts, q = problem(fam, n, seed)
+        tc = Treecode(pts, degree=12, cluster_size=leaf, theta=theta, eps=eps, kind=KIND_FIELD,
+                      degree_mode=DEGREE_PER_PAIR, degree_min=4)
+        X, E = selector.generate_samples(tc, q, per, K=K, seed=seed)
+        tc.close()
+        Xs.append(X)
+        Es.append(E)
+        log(f"{fam:8s} N={n} leaf={leaf} theta={theta}: {len(X)} samples ({time.time() - t0:.1f}s)")
+    return np.concatenate(Xs), np.concatenate(Es)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=selector.DEFAULT_WEIGHTS)
+    ap.add_argument("--samples", type=int, default=2_000_000)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--cache", default=None, help="sample cache (.npz); reused when present")
+    args = ap.parse_args()
+    cache = args.cache or os.path.splitext(args.out)[0] + "_samples.npz"
+    if os.path.exists(cache):
+        z = np.load(cache)
+        X, E = z["X"], z["E"]
+        print(f"loaded {len(X)} samples from {cache}")
+    else:
+        X, E = collect(args.samples)
+        np.savez(cache, X=X, E=E)
+    Y, M = selector.to_targets(E, 4, 12)
+    sel = selector.train(X, Y, M, epochs=args.epochs, batch=args.batch, lr=args.lr, log=print)
+    sel.meta.update({"families": ",".join(f"{f}:{n}:{l}:{t}" for f, n, l, t, _, _ in FAMILY)})
+    sel.save(args.out)
+    print(f"wrote {args.out}: {sel.meta}")
+
+
+if __name__ == "__main__":
+    main()
