@@ -1125,6 +1125,11 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     w.p[c] = P->d_ptw + (size_t)c * Pt * P->ipc;
     wm.p[c] = P->d_ptwm + (size_t)c * P->total_tgt_slots;
   }
+  cudaEvent_t ek[2];
+  for (auto& x : ek) BTK_CUDA(cudaEventCreate(&x));
+  BTK_CUDA(cudaEventRecord(ek[0], st));
+  BTK_CUDA(cudaEventRecord(ek[1], st));
+  bool first = true;
   auto solve = [&](const InteractCtx& ctx) -> btk_status {
     BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
                               S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
@@ -1138,7 +1143,9 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     BTK_CUDA(cudaMemsetAsync(P->d_ptw, 0, sizeof(double) * (size_t)P->ncomp * Pt * P->ipc, st));
     BTK_CUDA(cudaMemsetAsync(P->d_ptwm, 0, sizeof(double) * (size_t)P->ncomp * P->total_tgt_slots, st));
     BTK_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)P->ncomp * T.n_points, st));
-    BTK_TRY(run_interactions(ctx, P->d_S4, P->d_T4, P->d_T_out, o, wm, st));
+    BTK_TRY(run_interactions(ctx, P->d_S4, P->d_T4, P->d_T_out, o, wm, st, first ? ek[0] : nullptr,
+                             first ? ek[1] : nullptr));
+    first = false;
     BTK_CUDA(launch_promote(P->dim, P->degree, P->ncomp, (int)T.clusters.size(), P->d_t_cluster_panel,
                             P->d_t_cluster_slot_begin, P->d_t_slot_deg, P->d_t_slot_off, P->d_amat, P->d_amat_off,
                             wm, w, st));
@@ -1191,8 +1198,10 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     cudaEventElapsedTime(&report->ms_solve, e[1], e[2]);
     cudaEventElapsedTime(&report->ms_total, e[0], e[3]);
     std::memcpy(report->degree_hist, hist, sizeof(hist));
+    cudaEventElapsedTime(&report->ms_kernel, ek[0], ek[1]);
   }
   for (auto& x : e) cudaEventDestroy(x);
+  for (auto& x : ek) cudaEventDestroy(x);
   return check_status_word(P->ictx.d_ticket_status + 1, st);
 }
 

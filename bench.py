@@ -232,109 +232,176 @@ def load_traffic(key):
         return None
 
 
-def run_native(args, world, rank, local):
+class Form:
+    """One way of solving the workload: plain FP64 fixed degree (the reference
+    method), mixed precision fixed degree, or learned degrees + mixed."""
+
+    def __init__(self, name, pts, args):
+        import barytreek_b200 as btk
+        from barytreek_b200 import selector
+        self.name = name
+        kind = args.kind
+        self.sel = None
+        if name == "plain":
+            self.tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind,
+                                   precision=btk.PREC_FP64)
+        elif name == "mixed":
+            self.tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind,
+                                   precision=btk.PREC_MIXED)
+        else:
+            self.tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind,
+                                   precision=btk.PREC_MIXED, degree_mode=btk._lib.DEGREE_PER_PAIR, degree_min=4)
+            self.sel = selector.Selector.load()
+        self.report = None
+
+    def step(self, qd, out=None, coords=None):
+        """One solve; returns (total ms, interaction-kernel ms, evaluations)."""
+        tc = self.tc
+        if coords is not None:  # e2e: fresh device inputs
+            tc._t = tc._s = coords
+        if self.sel is None:
+            out = tc.solve(qd, out)
+            t = tc.last_timing()
+            return out, t["total"], t["interaction_kernel"], tc.evals(), t
+        out, rep = tc.solve_learned(qd, self.sel, tol=TOL, pair_tol=TOL * PAIR_TOL_FACTOR, degree_lo=4, out=out)
+        self.report = rep
+        return out, rep["ms_total"], rep["ms_kernel"], rep["evals_near"] + rep["evals_far"], rep
+
+
+TOL = 1e-6
+PAIR_TOL_FACTOR = 0.2
+
+
+def time_form(form, qd, flush, args, world, local):
     import torch
-    import barytreek_b200 as btk
-    from barytreek_b200 import _lib, datagen
+    from barytreek_b200 import _lib
     L = _lib.load()
-    kind, precision = args.kind, args.precision
-    pts, q = datagen.uniform_box(SEED, N_POINTS, 3, 0.0, 1.0)
-    t0 = time.time()
-    tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind, precision=precision)
-    torch.cuda.synchronize()
-    setup_s = time.time() - t0
-    evals = tc.evals()
-    qd = torch.from_numpy(q).cuda()
-    flush = torch.empty(32 << 20, dtype=torch.float64, device="cuda")  # 256 MB > 126 MB L2
     for _ in range(args.warmup):
-        tc.solve(qd)
-        tc.last_timing()
+        form.step(qd)
     barrier(world)
     torch.cuda.synchronize()
     launches0 = L.btk_launch_count()
-    step_ms, kern_ms, phases = [], [], []
+    tot, kern, evals, info = [], [], [], []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush_l2(flush)
             torch.cuda.synchronize()
-            out = tc.solve(qd)
-            t = tc.last_timing()
-            step_ms.append(t["total"])
-            kern_ms.append(t["interaction_kernel"])
-            phases.append(t)
+            out, t, k, e, extra = form.step(qd)
+            tot.append(t)
+            kern.append(k)
+            evals.append(e)
+            info.append(extra)
         torch.cuda.synchronize()
     launches = (L.btk_launch_count() - launches0) / max(1, args.steps)
-    clocks = clk.summary()
-    total_ms = sum(step_ms)
-    barrier(world)
-    total_ms_max = max_over_ranks(total_ms, world)
-    ms_per_step = total_ms_max / args.steps
-    value = world * evals / (ms_per_step * 1e-3)
+    total = max_over_ranks(sum(tot), world)
+    return {"ms": total / args.steps, "kernel_ms": statistics.mean(kern), "evals": statistics.mean(evals),
+            "launches": launches, "clocks": clk.summary(), "out": out, "info": info[-1]}
 
-    # e2e through the C ABI: pinned host inputs -> device, solve, results -> host.
+
+def run_native(args, world, rank, local):
+    import torch
+    from barytreek_b200 import _lib, datagen, selector
+    L = _lib.load()
+    kind = args.kind
+    pts, q = datagen.uniform_box(SEED, N_POINTS, 3, 0.0, 1.0)
+    qd = torch.from_numpy(q).cuda()
+    flush = torch.empty(32 << 20, dtype=torch.float64, device="cuda")  # 256 MB > 126 MB L2
+    headline = args.form
+    if headline == "learned" and not os.path.exists(selector.DEFAULT_WEIGHTS):
+        headline = "mixed"
+    names = ["plain", "mixed", "learned"] if headline == "learned" else sorted({"plain", headline})
+    results, forms = {}, {}
+    for name in names:
+        t0 = time.time()
+        forms[name] = Form(name, pts, args)
+        torch.cuda.synchronize()
+        setup = time.time() - t0
+        results[name] = time_form(forms[name], qd, flush, args, world, local)
+        results[name]["setup_s"] = setup
+    plain_evals = forms["plain"].tc.evals()
+    H = results[headline]
+    ms_per_step = H["ms"]
+    value = world * plain_evals / (ms_per_step * 1e-3)
+
+    # e2e through the C ABI for the headline form: pinned host coordinates and
+    # charges -> device, solve, results -> host, all inside the timed region.
+    f = forms[headline]
     h_in = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (*pts, q)]
     d_in = [torch.empty_like(a, device="cuda") for a in h_in]
-    h_out = torch.empty((tc.ncomp, tc.nt), dtype=torch.float64).pin_memory()
-    d_out = torch.empty((tc.ncomp, tc.nt), dtype=torch.float64, device="cuda")
+    h_out = torch.empty((f.tc.ncomp, f.tc.nt), dtype=torch.float64).pin_memory()
+    d_out = torch.empty((f.tc.ncomp, f.tc.nt), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2e_ms = []
+    keep = (f.tc._t, f.tc._s)
     for i in range(args.warmup + args.steps):
         flush_l2(flush)
         torch.cuda.synchronize()
         e0.record(stream)
         for h, d in zip(h_in, d_in):
             d.copy_(h, non_blocking=True)
-        _lib.check(L.btk_plan_execute(tc._plan, _lib.ptr(d_in[0]), _lib.ptr(d_in[1]), _lib.ptr(d_in[2]),
-                                      _lib.ptr(d_in[0]), _lib.ptr(d_in[1]), _lib.ptr(d_in[2]), _lib.ptr(d_in[3]),
-                                      _lib.ptr(d_out), stream.cuda_stream))
+        f.step(d_in[3], d_out, coords=d_in[:3])
         h_out.copy_(d_out, non_blocking=True)
         e1.record(stream)
         e1.synchronize()
         if i >= args.warmup:
             e2e_ms.append(e0.elapsed_time(e1))
+    f.tc._t, f.tc._s = keep
     e2e_total = max_over_ranks(sum(e2e_ms), world)
-    e2e_value = world * evals / (e2e_total / args.steps * 1e-3)
+    e2e_value = world * plain_evals / (e2e_total / args.steps * 1e-3)
     h2d = sum(h.numel() * h.element_size() for h in h_in)
     d2h = h_out.numel() * h_out.element_size()
-    ref_out = out.cpu().numpy()
-    assert np.linalg.norm(h_out.numpy() - ref_out) <= 1e-13 * np.linalg.norm(ref_out)
+    ref_out = H["out"].cpu().numpy()
+    assert np.linalg.norm(h_out.numpy() - ref_out) <= 1e-6 * np.linalg.norm(ref_out)
 
     if rank != 0:
         return None
-    # accuracy against the FP64 direct sum on a seeded 10k-target subsample
-    idx, ds = direct_check(tc, q, kind)
-    o = out.cpu().numpy()[:, idx]
-    acc = [float(np.linalg.norm(o[c] - ds[c]) / np.linalg.norm(ds[c])) for c in range(tc.ncomp)]
-    acc_all = float(np.linalg.norm(o - ds) / np.linalg.norm(ds))
-    # roofline of the dominant kernel against the live-measured FP64 FMA pipe peak
+    idx, ds = direct_check(f.tc, q, kind)
+    acc = {}
+    for name in names:
+        o = results[name]["out"].cpu().numpy()[:, idx]
+        acc[name] = float(np.linalg.norm(o - ds) / np.linalg.norm(ds))
+    per_comp = [float(np.linalg.norm(H["out"].cpu().numpy()[c, idx] - ds[c]) / np.linalg.norm(ds[c]))
+                for c in range(ds.shape[0])]
     peak = ctypes.c_double()
-    _lib.check(L.btk_measure_pipe_peak(0 if precision == 0 else 1, ctypes.byref(peak), None))
-    kernel_ms = statistics.mean(kern_ms)
-    flops = FLOPS_PER_EVAL[kind] * evals
+    fp32 = headline != "plain"
+    _lib.check(L.btk_measure_pipe_peak(1 if fp32 else 0, ctypes.byref(peak), None))
+    kernel_ms = H["kernel_ms"]
+    flops = FLOPS_PER_EVAL[kind] * H["evals"]
     achieved = flops / (kernel_ms * 1e-3) / 1e12
-    traffic = load_traffic(f"interact_fp64_k{kind}_cfg2")
+    kname = "k_interact_mixed" if fp32 else "k_interact_fp64"
     line = {
         "metric": METRIC, "value": value, "unit": "interactions/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if precision == 0 else "f32+f64",
+        "vs_baseline": None, "dtype": "f64" if headline == "plain" else "f32+f64",
         "data": "synthetic: seeded SplitMix64, uniform unit cube, charges U[-1,1]",
-        "config": {"workload": workload_name(kind, precision), "l2": "flushed (256 MB write) before every step",
-                   "parallelism": "replicas" if world > 1 else "single GPU", "interactions_per_solve": evals,
-                   "evals_by_class": {k: v for k, v in tc.stats().items() if k.startswith("evals")}},
-        "roofline": {"bound": "fp64" if precision == 0 else "fp32", "achieved": achieved, "peak": peak.value,
-                     "unit": "TFLOP/s", "frac": achieved / peak.value, "traffic": traffic,
-                     "kernel": "k_interact_fp64 (persistent PP/PC/CP/CC)", "kernel_ms": kernel_ms,
-                     "flops_per_launch": flops,
-                     "peak_source": "measured live: btk_measure_pipe_peak FMA-chain probe on this GPU"},
+        "config": {"workload": workload_name(kind, 0 if headline == "plain" else 1) +
+                   (", learned per-pair degrees 4..8 with 1% direct-sum audit" if headline == "learned" else ""),
+                   "form": headline, "tolerance_rel_l2": TOL,
+                   "value_definition": "interactions of the plain fixed-degree solve of this workload "
+                                       "(pairwise evaluations at n=8) divided by the solve time of the reported form",
+                   "l2": "flushed (256 MB write) before every step",
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "interactions_plain": plain_evals, "interactions_evaluated": H["evals"]},
+        "forms": {n: {"ms_per_step": r["ms"], "interaction_kernel_ms": r["kernel_ms"], "evaluations": r["evals"],
+                      "rel_l2_vs_direct_10k": acc[n], "setup_s": r["setup_s"],
+                      "speedup_vs_plain_fp64": results["plain"]["ms"] / r["ms"]} for n, r in results.items()},
+        "roofline": {"bound": "fp32" if fp32 else "fp64", "achieved": achieved, "peak": peak.value,
+                     "unit": "TFLOP/s", "frac": achieved / peak.value,
+                     "traffic": load_traffic(f"{kname}_k{kind}_cfg2"), "kernel": f"{kname} (persistent PP/PC/CP/CC)",
+                     "kernel_ms": kernel_ms, "flops_per_launch": flops,
+                     "peak_source": "measured live: btk_measure_pipe_peak FMA-chain probe on this GPU "
+                                    f"({'FP32' if fp32 else 'FP64'} pipe)"},
         "e2e": {"value": e2e_value, "unit": "interactions/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_total / args.steps},
-        "gpu_launches": launches,
-        "clocks": clocks,
-        "accuracy": {"rel_l2_vs_direct_10k": acc_all, "per_component": acc},
-        "phases_ms": {k: statistics.mean(p[k] for p in phases) for k in phases[0]},
-        "setup_s": setup_s,
+        "gpu_launches": H["launches"],
+        "clocks": H["clocks"],
+        "accuracy": {"rel_l2_vs_direct_10k": acc[headline], "per_component": per_comp},
     }
+    if headline == "learned":
+        r = forms["learned"].report
+        line["learned"] = {k: r[k] for k in ("audit_rel_l2", "audit_targets", "fell_back", "evals_near", "evals_far",
+                                             "ms_select", "ms_solve", "ms_kernel", "degree_hist")}
     if world == 1 and not args.no_cpu_baseline:
         from oracle import RefLib
         if RefLib.available():
@@ -348,7 +415,8 @@ def run_native(args, world, rank, local):
                 "est_solve_s": r["est_solve_s"]}
         else:
             line["cpu_baseline"] = None
-    tc.close()
+    for fm in forms.values():
+        fm.tc.close()
     return line
 
 
@@ -359,7 +427,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--kind", type=int, default=2, choices=[0, 2])
-    ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
+    ap.add_argument("--form", default="learned", choices=["plain", "mixed", "learned"],
+                    help="the form reported as the headline (all cheaper forms are timed beside it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=N_POINTS, help="point count (profiling captures only)")
     args = ap.parse_args()

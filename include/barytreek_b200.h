@@ -352,6 +352,7 @@ typedef struct {
   float ms_solve;      /* interactions + promotion + downward at the chosen degrees */
   float ms_total;      /* everything, audit and fallback included */
   int degree_hist[13]; /* far-field pairs per chosen degree */
+  float ms_kernel;     /* the interaction kernel of the learned solve alone */
 } btk_learned_report;
 
 /* Learned-degree solve: upward pass, features, network, per-pair degree =
