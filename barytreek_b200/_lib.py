@@ -115,7 +115,7 @@ SIGNATURES = {
     "btk_plan_pair_count": [_vp, _vp],
     "btk_plan_pair_features": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_plan_execute_learned": [_vp, _vp, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
-    "btk_plan_error_samples": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _ci, _vp, _ci, _vp, _vp, _vp, _vp, _vp],
+    "btk_plan_error_samples": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _ci, _vp, _ci, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_mlp_forward": [_vp, _ci, _vp, _vp, _vp],
     "btk_mlp_gradient": [_vp, _ci, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_mlp_adam": [_vp, _vp, _vp, _vp, _vp, _ci, ctypes.c_float, _vp],

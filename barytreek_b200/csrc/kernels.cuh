@@ -135,13 +135,14 @@ struct SampleArgs {
   int slot_d_lo;
   double* exact;   // [n][K][ncomp]
   double* approx;  // [n][n_deg][K][ncomp]
+  const double* ref;  // optional [ncomp][nt] total solution: errors relative to it
 };
 cudaError_t launch_error_samples(const SampleArgs& a, float* log10_err, cudaStream_t s);
 int selector_param_count();
 cudaError_t launch_panel_desc(int dim, int n, int P, const double* psw, float* desc, cudaStream_t s);
 cudaError_t launch_pair_features(int n_pairs, const int* ptype, const int* ptgt, const int* psrc, const DevPanel* pt,
-                                 const DevPanel* ps, double root_radius, double eps, const float* desc_s, float* feat,
-                                 cudaStream_t s);
+                                 const DevPanel* ps, double root_radius, double eps, const float* desc_s,
+                                 int n_points, const double4* pts, double* gsum, float* feat, cudaStream_t s);
 cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const float* feat, float* out,
                              cudaStream_t s);
 cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int* deg,

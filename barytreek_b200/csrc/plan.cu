@@ -513,6 +513,7 @@ struct btk_plan {
   float *d_desc = nullptr, *d_feat = nullptr, *d_pred = nullptr;
   unsigned long long* d_evals = nullptr;
   int* d_hist = nullptr;
+  double* d_gsum = nullptr;  // sum |q|, sum q
   double root_radius = 1.0, root_centre[3] = {0, 0, 0};
   // audit: a fixed 1% sample of the targets, direct sum over all sources
   int n_audit = 0;
@@ -737,6 +738,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     BTK_TRY(A.alloc(&P->d_pred, (size_t)std::max(P->n_pairs, 1) * 9));
     BTK_TRY(A.alloc(&P->d_evals, 1));
     BTK_TRY(A.alloc(&P->d_hist, kMaxNodes));
+    BTK_TRY(A.alloc(&P->d_gsum, 2));
     BTK_TRY(A.upload(&P->d_cluster_slot_s, S.cluster_slot));
     BTK_TRY(A.upload(&P->d_cluster_slot_t, T.cluster_slot));
     const PanelGeom& g = S.h.geom[0];
@@ -1088,7 +1090,8 @@ btk_status btk_plan_pair_features(btk_plan* P, const double* xs, const double* y
   BTK_TRY(run_upward(S, P->d_S4, P->d_psw, st));
   BTK_CUDA(launch_panel_desc(P->dim, P->degree, S.h.panel_count, P->d_psw, P->d_desc, st));
   BTK_CUDA(launch_pair_features(P->n_pairs, P->d_pair_type, P->d_pair_tgt, P->d_pair_src, P->tgt.d_panels,
-                                S.d_panels, P->root_radius, P->eps, P->d_desc, features, st));
+                                S.d_panels, P->root_radius, P->eps, P->d_desc, S.n_points, P->d_S4, P->d_gsum,
+                                features, st));
   return BTK_OK;
 }
 
@@ -1208,7 +1211,8 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
 btk_status btk_plan_error_samples(btk_plan* P, const double* xt, const double* yt, const double* zt,
                                   const double* xs, const double* ys, const double* zs, const double* charges, int n,
                                   const int* pair_index, int K, const int* target_orig, const int* src_leaf_csr,
-                                  const int* src_leaves, float* log10_err, btk_stream_t stream) {
+                                  const int* src_leaves, const double* ref, float* log10_err,
+                                  btk_stream_t stream) {
   BTK_CHECK(P && xt && yt && xs && ys && charges && (P->dim == 2 || (zt && zs)), BTK_ERR_INVALID_ARGUMENT,
             "btk_plan_error_samples: null argument");
   BTK_CHECK(P->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT, "plan is not BTK_DEGREE_PER_PAIR");
@@ -1282,6 +1286,7 @@ btk_status btk_plan_error_samples(btk_plan* P, const double* xt, const double* y
   a.slot_d_lo = P->degree_min;
   a.exact = d_exact;
   a.approx = d_approx;
+  a.ref = ref;
   BTK_CUDA(launch_error_samples(a, d_err, st));
   BTK_CUDA(cudaMemcpyAsync(log10_err, d_err, sizeof(float) * (size_t)n * n_deg, cudaMemcpyDeviceToHost, st));
   BTK_CUDA(cudaStreamSynchronize(st));

@@ -104,9 +104,34 @@ __global__ void __launch_bounds__(256) k_panel_desc(int dim, int n, int P, const
 
 // ---- per-pair features -------------------------------------------------------
 // type: 1 PC, 2 CP, 3 CC. Pairs listed PC, then CP, then CC.
+// Sum |q| and sum q over the sources (the global potential scale and net
+// charge the features are normalised by).
+__global__ void k_global_sums(int n, const double4* pts, double* sums) {
+  double a = 0.0, b = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    a += fabs(pts[i].w);
+    b += pts[i].w;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, off);
+    b += __shfl_down_sync(0xffffffffu, b, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(sums, a);
+    atomicAdd(sums + 1, b);
+  }
+}
+
+// Features of pair i:
+//  0 log10(r_T/R)  1 log10(r_S/R)  2 log10(d/(r_T+r_S))  3 log10(d/r_S)
+//  4 log10(d/r_T)  5 log10(1+m_T)  6 log10(1+m_S)  7-9 class (PC, CP, CC)
+// 10 log10(eps/d)  11 source net-charge fraction  12, 13 source Chebyshev-
+// moment energy in bands 3-4 and >=7  14 log10((sum|W_S|/d) / (sum|q|/R)):
+// the pair's potential scale against the global one  15 global net-charge
+// fraction log10(|sum q| / sum |q|). R = root radius, d = centre distance.
 __global__ void k_pair_features(int n_pairs, const int* ptype, const int* ptgt, const int* psrc,
                                 const DevPanel* pt, const DevPanel* ps, double root_radius, double eps,
-                                const float* desc_s, float* feat) {
+                                const float* desc_s, const double* gsum, float* feat) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_pairs) return;
   const DevPanel T = pt[ptgt[i]], S = ps[psrc[i]];
@@ -132,7 +157,12 @@ __global__ void k_pair_features(int n_pairs, const int* ptype, const int* ptgt, 
   f[9] = ptype[i] == 3 ? 1.f : 0.f;
   f[10] = lg(eps / dist + 1e-12);
   const float* d = desc_s + (size_t)psrc[i] * kDescs;
-  for (int q = 0; q < 5; ++q) f[11 + q] = d[1 + q];
+  f[11] = d[1];
+  f[12] = d[3];
+  f[13] = d[5];
+  const double g_abs = gsum[0] > 1e-300 ? gsum[0] : 1e-300;
+  f[14] = d[0] - lg(dist) - lg(g_abs / root_radius);
+  f[15] = lg(fabs(gsum[1]) / g_abs + 1e-16);
 }
 
 // ---- MLP ----------------------------------------------------------------------
@@ -497,19 +527,24 @@ __global__ void __launch_bounds__(256) k_sample_approx(SampleArgs a) {
   }
 }
 
-// log10 of the relative L2 error of each degree against the exact values.
+// log10 of each degree's L2 error at the sample's targets, relative to the L2
+// norm of `ref` there (ref = [ncomp][nt] total solution in original order) or,
+// without ref, to the pair's exact contribution.
 __global__ void k_sample_errors(int n, int n_deg, int K, int ncomp, const double* exact, const double* approx,
-                                float* out) {
+                                const double* ref, int nt, const int* tgt_orig, float* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n * n_deg) return;
   const int s = i / n_deg, di = i % n_deg;
   double e = 0.0, r = 0.0;
-  for (int q = 0; q < K * ncomp; ++q) {
-    const double x = exact[(size_t)s * K * ncomp + q];
-    const double y = approx[((size_t)s * n_deg + di) * K * ncomp + q];
-    e += (x - y) * (x - y);
-    r += x * x;
-  }
+  for (int k = 0; k < K; ++k)
+    for (int c = 0; c < ncomp; ++c) {
+      const int q = k * ncomp + c;
+      const double x = exact[(size_t)s * K * ncomp + q];
+      const double y = approx[((size_t)s * n_deg + di) * K * ncomp + q];
+      e += (x - y) * (x - y);
+      const double rv = ref ? ref[(size_t)c * nt + tgt_orig[(size_t)s * K + k]] : x;
+      r += rv * rv;
+    }
   out[i] = (float)log10(sqrt(e / (r > 1e-300 ? r : 1e-300)) + 1e-30);
 }
 
@@ -554,7 +589,8 @@ cudaError_t launch_error_samples(const SampleArgs& a, float* log10_err, cudaStre
     k_sample_approx<3><<<a.n * a.n_deg, 256, shm, s>>>(a);
   }
   const int m = a.n * a.n_deg;
-  k_sample_errors<<<(m + 255) / 256, 256, 0, s>>>(a.n, a.n_deg, a.K, a.ncomp, a.exact, a.approx, log10_err);
+  k_sample_errors<<<(m + 255) / 256, 256, 0, s>>>(a.n, a.n_deg, a.K, a.ncomp, a.exact, a.approx, a.ref, (int)a.nt,
+                                                  a.tgt_orig, log10_err);
   count_launch(3);
   return cudaGetLastError();
 }
@@ -574,11 +610,17 @@ cudaError_t launch_panel_desc(int dim, int n, int P, const double* psw, float* d
 }
 
 cudaError_t launch_pair_features(int n_pairs, const int* ptype, const int* ptgt, const int* psrc, const DevPanel* pt,
-                                 const DevPanel* ps, double root_radius, double eps, const float* desc_s, float* feat,
-                                 cudaStream_t s) {
-  if (n_pairs <= 0) return cudaSuccess;
+                                 const DevPanel* ps, double root_radius, double eps, const float* desc_s,
+                                 int n_points, const double4* pts, double* gsum, float* feat, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(gsum, 0, 2 * sizeof(double), s);
+  if (e != cudaSuccess) return e;
+  if (n_points > 0) {
+    k_global_sums<<<296, 256, 0, s>>>(n_points, pts, gsum);
+    count_launch();
+  }
+  if (n_pairs <= 0) return cudaGetLastError();
   k_pair_features<<<(n_pairs + 127) / 128, 128, 0, s>>>(n_pairs, ptype, ptgt, psrc, pt, ps, root_radius, eps, desc_s,
-                                                        feat);
+                                                        gsum, feat);
   count_launch();
   return cudaGetLastError();
 }

@@ -107,6 +107,10 @@ def generate_samples(tc, charges, n_samples: int, K: int = 32, seed: int = 0, ba
     stream = torch.cuda.current_stream(tc.device).cuda_stream
     check(L.btk_plan_pair_features(tc._plan, ptr(s[0]), ptr(s[1]), zs, ptr(q), ptr(feat), stream))
     feat = feat.cpu().numpy()
+    # The total solution at the plan degree (every pair at the highest degree):
+    # pair errors are measured relative to it, which is what the global
+    # tolerance constrains.
+    ref = tc.solve(q)
     # pair table (PC, CP, CC) -> (target, source panels)
     pp, pc, cp, cc = tc.lists
     tg = np.concatenate([pc["target_panel"], cp["target_panel"], cc["target_panel"]])
@@ -142,7 +146,8 @@ def generate_samples(tc, charges, n_samples: int, K: int = 32, seed: int = 0, ba
         out = np.zeros((len(idx), n_deg), np.float32)
         pi = np.ascontiguousarray(idx, np.int32)
         check(L.btk_plan_error_samples(tc._plan, ptr(tc._t[0]), ptr(tc._t[1]), zt, ptr(s[0]), ptr(s[1]), zs, ptr(q),
-                                       len(idx), ptr(pi), K, ptr(tgt_orig), ptr(csr), ptr(leaves), ptr(out), stream))
+                                       len(idx), ptr(pi), K, ptr(tgt_orig), ptr(csr), ptr(leaves), ptr(ref), ptr(out),
+                                       stream))
         errs[b0:b0 + len(idx)] = out
     return feat[pick], errs
 

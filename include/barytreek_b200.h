@@ -374,11 +374,14 @@ btk_status btk_plan_execute_learned(btk_plan* plan, const btk_selector* sel, dou
  * d = degree_min..interp_degree, against the FP64 direct sum over the points
  * under the pair's source panel (src_leaf_csr[n+1] / src_leaves: the leaf
  * panels under each source). Coordinates and charges are device arrays as in
- * btk_plan_execute. log10_err: host float [n][interp_degree - degree_min + 1]. */
+ * btk_plan_execute. ref (optional, device [ncomp][point_count_target], original
+ * order): when given, each error is relative to the L2 norm of ref at the
+ * sample's targets (the total solution there) instead of to the pair's own
+ * contribution. log10_err: host float [n][interp_degree - degree_min + 1]. */
 btk_status btk_plan_error_samples(btk_plan* plan, const double* xt, const double* yt, const double* zt,
                                   const double* xs, const double* ys, const double* zs, const double* charges, int n,
                                   const int* pair_index, int K, const int* target_orig, const int* src_leaf_csr,
-                                  const int* src_leaves, float* log10_err, btk_stream_t stream);
+                                  const int* src_leaves, const double* ref, float* log10_err, btk_stream_t stream);
 
 /* Training kernels (device arrays). Inputs xn are normalised features
  * [n][16], targets tn normalised [n][9], mask [n][9] (0/1). */
