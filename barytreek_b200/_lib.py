@@ -100,6 +100,7 @@ SIGNATURES = {
     "btk_downward_pass_3d": [_PRC, _PTI, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _ci, _vp],
     "btk_downward_pass_3d_3": [_PRC, _PTI, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _ci, _vp],
     "btk_direct_sum": [_ci, _ci, _cd, _ci, _vp, _vp, _vp, _ci, _vp, _vp, _vp, _vp, _vp, _vp],
+    "btk_direct_sum_noalloc": [_ci, _ci, _cd, _ci, _vp, _vp, _vp, _ci, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_plan_create": [_vp, ctypes.POINTER(PlanDesc), _vp],
     "btk_plan_destroy": [_vp],
     "btk_plan_stats_get": [_vp, ctypes.POINTER(PlanStats)],

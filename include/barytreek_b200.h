@@ -231,6 +231,21 @@ btk_status btk_direct_sum(int dim, int kind, double eps, int nt, const double* x
                           const double* zt, int ns, const double* xs, const double* ys, const double* zs,
                           const double* charges, double* out, btk_stream_t stream);
 
+/* btk_direct_sum without any device allocation. No counterpart in the
+ * reference. Same arguments and bit-identical results; its scratch (the
+ * packed sources) lives in a static device array, so ns is limited to
+ * 262,144 (BTK_ERR_INVALID_ARGUMENT above that). For callers that cannot
+ * allocate during the call: a host whose caching allocator has reserved the
+ * device memory, or a time-stepping loop that cannot pay an allocation every
+ * step. Returns once the work is enqueued on `stream` (on the current
+ * device). One scratch per device: overlapping calls on one device (threads,
+ * or streams not ordered against each other) race. The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress); make it before
+ * any stream capture begins on that device. */
+btk_status btk_direct_sum_noalloc(int dim, int kind, double eps, int nt, const double* xt, const double* yt,
+                                  const double* zt, int ns, const double* xs, const double* ys, const double* zs,
+                                  const double* charges, double* out, btk_stream_t stream);
+
 /* ---- 3. Plan API ------------------------------------------------------ */
 
 /* Kernel kinds. POT is the reference potential (2-D +(1/4pi)log(r^2+eps^2),
