@@ -120,7 +120,7 @@ def generate_samples(tc, charges, n_samples: int, K: int = 32, seed: int = 0, ba
     valid = np.flatnonzero((tt.panels["point_count"][tg] > 0) & (st.panels["point_count"][sr] > 0))
     if len(valid) == 0:
         return np.zeros((0, N_FEATURES), np.float32), np.zeros((0, 0), np.float32)
-    pick = valid[rng.choice(len(valid), size=min(n_samples, len(valid)), replace=n_samples > len(valid))]
+    pick = valid[rng.choice(len(valid), size=min(n_samples, len(valid)), replace=False)]
     n_deg = tc.cfg.interp_degree - tc.degree_min + 1
     errs = np.zeros((len(pick), n_deg), np.float32)
     leaves_cache_t, leaves_cache_s = {}, {}

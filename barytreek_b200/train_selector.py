@@ -51,6 +51,8 @@ def problem(family, n, seed):
 
 
 def collect(n_total, K=16, log=print, max_rounds=12):
+    # at most this many pairs from one problem, so every family contributes
+    per_problem = max(20000, n_total // (2 * len(BASE)))
     Xs, Es, got = [], [], 0
     for r in range(max_rounds):
         for i, (fam, n, leaf, theta, eps) in enumerate(BASE):
@@ -61,7 +63,7 @@ def collect(n_total, K=16, log=print, max_rounds=12):
             pts, q = problem(fam, n, seed)
             tc = Treecode(pts, degree=12, cluster_size=leaf, theta=theta, eps=eps, kind=KIND_FIELD,
                           degree_mode=DEGREE_PER_PAIR, degree_min=4)
-            X, E = selector.generate_samples(tc, q, n_total - got, K=K, seed=seed)
+            X, E = selector.generate_samples(tc, q, min(per_problem, n_total - got), K=K, seed=seed)
             tc.close()
             Xs.append(X)
             Es.append(E)

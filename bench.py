@@ -269,7 +269,7 @@ class Form:
 
 
 TOL = 1e-6
-PAIR_TOL_FACTOR = 0.05
+PAIR_TOL_FACTOR = 0.1
 
 
 def time_form(form, qd, flush, args, world, local):
