@@ -59,13 +59,37 @@ class PlanDesc(ctypes.Structure):
                 ("point_leaf_panel_source", ctypes.c_void_p), ("pp_list", ctypes.c_void_p),
                 ("pc_list", ctypes.c_void_p), ("cp_list", ctypes.c_void_p), ("cc_list", ctypes.c_void_p),
                 ("kind", ctypes.c_int), ("precision", ctypes.c_int), ("degree_mode", ctypes.c_int),
-                ("degree_min", ctypes.c_int)]
+                ("degree_min", ctypes.c_int), ("work_split", ctypes.c_int)]
 
 
 class PlanStats(ctypes.Structure):
     _fields_ = [("evals_pp", ctypes.c_int64), ("evals_pc", ctypes.c_int64), ("evals_cp", ctypes.c_int64),
                 ("evals_cc", ctypes.c_int64), ("work_items", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
                 ("levels_target", ctypes.c_int), ("levels_source", ctypes.c_int)]
+
+
+class ForestDesc(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("degree", ctypes.c_int), ("theta", ctypes.c_double), ("eps", ctypes.c_double),
+                ("n_problems", ctypes.c_int), ("point_offset", ctypes.c_void_p), ("cluster_size", ctypes.c_void_p)]
+
+
+class Forest(ctypes.Structure):
+    _fields_ = [("cfg", RunConfig), ("info", TreeInfo), ("panels", ctypes.c_void_p),
+                ("point_leaf_panel", ctypes.c_void_p), ("panel_problem", ctypes.c_void_p),
+                ("panel_local", ctypes.c_void_p), ("pp_list", ctypes.c_void_p), ("pc_list", ctypes.c_void_p),
+                ("cp_list", ctypes.c_void_p), ("cc_list", ctypes.c_void_p)]
+
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [("forest", ForestDesc), ("kind", ctypes.c_int), ("precision", ctypes.c_int),
+                ("work_split", ctypes.c_int)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("n_problems", ctypes.c_int), ("total_points", ctypes.c_int64), ("panel_count", ctypes.c_int),
+                ("levels", ctypes.c_int), ("evals_pp", ctypes.c_int64), ("evals_pc", ctypes.c_int64),
+                ("evals_cp", ctypes.c_int64), ("evals_cc", ctypes.c_int64), ("work_items", ctypes.c_int64),
+                ("graph_kernel_nodes", ctypes.c_int), ("graph_nodes", ctypes.c_int), ("last_ms", ctypes.c_float)]
 
 
 class BtkError(RuntimeError):
@@ -120,9 +144,15 @@ SIGNATURES = {
     "btk_mlp_forward": [_vp, _ci, _vp, _vp, _vp],
     "btk_mlp_gradient": [_vp, _ci, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_mlp_adam": [_vp, _vp, _vp, _vp, _vp, _ci, ctypes.c_float, _vp],
+    "btk_forest_build": [ctypes.POINTER(ForestDesc), _vp, _vp, _vp, ctypes.POINTER(Forest)],
+    "btk_forest_free": [ctypes.POINTER(Forest)],
+    "btk_batch_create": [_vp, ctypes.POINTER(BatchDesc), _vp, _vp, _vp, _vp],
+    "btk_batch_destroy": [_vp],
+    "btk_batch_execute": [_vp, _vp, _vp, _vp],
+    "btk_batch_stats_get": [_vp, ctypes.POINTER(BatchStats)],
 }
 _RESTYPES = {"btk_last_error": ctypes.c_char_p, "btk_version": ctypes.c_char_p, "btk_launch_count": ctypes.c_uint64,
-             "btk_free": None, "btk_selector_weights": ctypes.c_void_p}
+             "btk_free": None, "btk_selector_weights": ctypes.c_void_p, "btk_forest_free": None}
 
 
 class LearnedReport(ctypes.Structure):

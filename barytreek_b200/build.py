@@ -24,7 +24,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.pat
 # trees and lists): no contraction into fused multiply-adds.
 PER_FILE = {"host_tree.cpp": ["-Xcompiler", "-ffp-contract=off"]}
 SOURCES = ["host_tree.cpp", "plan.cu", "kernels_updown.cu", "kernels_interact.cu", "kernels_direct.cu",
-           "kernels_probe.cu", "kernels_degree.cu", "selector.cu", "direct_noalloc.cu"]
+           "kernels_probe.cu", "kernels_degree.cu", "selector.cu", "direct_noalloc.cu", "batch.cpp"]
 HEADERS = ["btk_internal.h", "kernels.cuh", "device_math.cuh"]
 
 

@@ -39,7 +39,7 @@ struct WorkItem {
   int t_count;         // targets in this tile
   int e_begin, e_end;  // entry range
   int s_total;         // sources over the entries
-  int flags;           // kItemProxyTargets | kItemAtomic
+  int flags;           // kItemProxyTargets | kItemAtomic | kItemAudit
   int near_total;      // the first near_total sources are PP (near-field) points
   int pad1;
   double cx, cy, cz;   // FP64 centre of the target panel (mixed precision origin)
@@ -48,6 +48,7 @@ struct WorkItem {
 static_assert(sizeof(WorkItem) == 64, "WorkItem is one 64-byte record");
 constexpr int kItemProxyTargets = 1;  // outputs go to proxy target weights
 constexpr int kItemAtomic = 2;        // another item shares these targets
+constexpr int kItemAudit = 4;         // direct-sum audit: targets T4a[t_begin + i], outputs aout[c][t_begin + i]
 
 struct Entry {
   int s_begin;  // first source in the S4 array
@@ -67,6 +68,8 @@ struct InteractParams {
   const int* T_out;
   double* out[4];  // point-target outputs, one per component
   double* ptw[4];  // proxy-target outputs, one per component
+  const double4* T4a;  // audit targets (kItemAudit items)
+  double* aout[4];     // audit outputs, one per component
   double eps2;
   double scale[4];
   int* ticket;
@@ -147,8 +150,10 @@ cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const
                              cudaStream_t s);
 cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int* deg,
                                   cudaStream_t s);
+// Far-field evaluations at the chosen degrees (summed into *evals) and the
+// histogram of the degrees (hist[0..12], added to).
 cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
-                             const int* cp_scount, unsigned long long* evals, cudaStream_t s);
+                             const int* cp_scount, unsigned long long* evals, int* hist, cudaStream_t s);
 cudaError_t launch_audit_compare(int n, int ncomp, int nt, const int* audit_sorted, const int* perm,
                                  const double* out, const double* audit_out, double* sums, cudaStream_t s);
 cudaError_t launch_fill_int(int n, int value, int* dst, cudaStream_t s);

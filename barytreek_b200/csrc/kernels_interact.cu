@@ -13,7 +13,9 @@
 // Per item, thread 0 streams the item's sources through a STAGES-deep ring of
 // shared-memory chunks with TMA bulk copies (cp.async.bulk, completion on an
 // mbarrier); all 128 threads evaluate their 2 targets against every source of a
-// chunk (broadcast shared-memory reads) and keep the sums in registers. Each
+// chunk (broadcast shared-memory reads) and keep the sums in registers. Warp w
+// owns targets [64 w, 64 w + 64) of a tile; warps whose targets lie past the
+// tile's count skip the arithmetic. Each
 // target's sum is written once at the end of its item, so results need no
 // atomics unless the host split a long source list (kItemAtomic).
 #include "device_math.cuh"
@@ -79,12 +81,14 @@ template <int DIM, int KIND, bool GUARD>
 __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractParams p) {
   constexpr int NC = KernelTraits<DIM, KIND>::NC;
   constexpr int TPT = kTargetsPerThread;
+  static_assert(TPT == 2, "targets of a warp are [64 w, 64 w + 64): two per thread");
   __shared__ __align__(128) double4 sbuf[kStages][kChunk];
   __shared__ __align__(8) uint64_t bars[kStages];
   __shared__ int s_item, s_abort;
   __shared__ uint32_t s_fail_chunk;
 
   const int tid = threadIdx.x;
+  const int lane = tid & 31, tbase = (tid >> 5) * 64;
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
@@ -131,11 +135,15 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
       for (int c = 0; c < min(kStages, n_chunks); ++c) issue(c);
     }
 
+    // This warp's targets: [tbase, tbase + 64) of the tile, nu of its two
+    // 32-target halves in use (warp-uniform), so a partly filled tile leaves
+    // its idle warps' issue slots to other blocks.
+    const int nu = w.t_count > tbase + 32 ? 2 : (w.t_count > tbase ? 1 : 0);
     double tx[TPT], ty[TPT], tz[TPT], acc[TPT][NC];
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int i = min(tid + u * kInteractThreads, w.t_count - 1);
-      const double4 t = p.T4[w.t_begin + i];
+      const int i = min(tbase + u * 32 + lane, w.t_count - 1);
+      const double4 t = ((w.flags & kItemAudit) ? p.T4a : p.T4)[w.t_begin + i];
       tx[u] = t.x;
       ty[u] = t.y;
       tz[u] = t.z;
@@ -155,11 +163,16 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
       if (s_abort) break;
       const int cnt = min(kChunk, w.s_total - c * kChunk);
       const double4* sb = sbuf[stage];
+      if (nu == 2) {
 #pragma unroll 2
-      for (int j = 0; j < cnt; ++j) {
-        const double4 s = sb[j];
-#pragma unroll
-        for (int u = 0; u < TPT; ++u) eval_fp64<DIM, KIND, GUARD>(tx[u], ty[u], tz[u], s, p.eps2, acc[u]);
+        for (int j = 0; j < cnt; ++j) {
+          const double4 s = sb[j];
+          eval_fp64<DIM, KIND, GUARD>(tx[0], ty[0], tz[0], s, p.eps2, acc[0]);
+          eval_fp64<DIM, KIND, GUARD>(tx[1], ty[1], tz[1], s, p.eps2, acc[1]);
+        }
+      } else if (nu == 1) {
+#pragma unroll 2
+        for (int j = 0; j < cnt; ++j) eval_fp64<DIM, KIND, GUARD>(tx[0], ty[0], tz[0], sb[j], p.eps2, acc[0]);
       }
       __syncthreads();
       if (tid == 0 && c + kStages < n_chunks) issue(c + kStages);
@@ -169,12 +182,13 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
 
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int i = tid + u * kInteractThreads;
+      const int i = tbase + u * 32 + lane;
       if (i < w.t_count) {
-        const int idx = p.T_out[w.t_begin + i];
+        const bool audit = (w.flags & kItemAudit) != 0;
+        const int idx = audit ? w.t_begin + i : p.T_out[w.t_begin + i];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          double* dst = ((w.flags & kItemProxyTargets) ? p.ptw[c] : p.out[c]) + idx;
+          double* dst = (audit ? p.aout[c] : (w.flags & kItemProxyTargets) ? p.ptw[c] : p.out[c]) + idx;
           const double v = acc[u][c] * p.scale[c];
           if (w.flags & kItemAtomic)
             atomicAdd(dst, v);
@@ -197,51 +211,93 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
 // Mixed precision: the same pipeline, but every chunk of FP64 sources is
 // rewritten in shared memory as FP32 coordinates relative to the item's FP64
 // target-panel centre (one FP64 subtraction per source per item), and the
-// pairwise arithmetic runs in FP32 with the MUFU approximations. Per target,
+// pairwise arithmetic runs in FP32 with the MUFU approximations. Sources are
+// stored as PAIRS (even, odd) in packed float2 lanes, negated, so one sm_100
+// f32x2 instruction (FADD2/FMUL2/FFMA2) evaluates a target against two
+// sources: half the issue slots of scalar FP32 for the same work. Per target,
 // FP32 partial sums over kFold sources are folded into an FP64 accumulator
 // with a compensated (two-sum) addition, so the final per-target sum carries
 // FP64 precision; the constant factor is applied in FP64 at the end.
 // ---------------------------------------------------------------------------
-constexpr int kFold = 128;
+constexpr int kPairs = kChunk / 2;   // source pairs per chunk
+constexpr int kFoldPairs = 64;       // fold FP32 partials into FP64 every 128 sources
+static_assert(kPairs == kInteractThreads, "one thread converts one source pair per chunk");
+// Padding source for an odd chunk: zero weight, placed 3e18 away (negated
+// relative coordinate), so r^2 stays finite in FP32 and the term is exactly 0.
+constexpr float kPadCoord = -3.0e18f;
 
-// NEAR: coordinates carry an FP32 low part (x = hi + lo, both relative to the
-// item's centre), and the difference is formed as (t_hi - s_hi) + (t_lo - s_lo)
-// so near-field pairs (PP) keep their separation to ~1e-14 relative to the
-// centre distance, not FP32's 6e-8.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// One target, both lanes holding the same coordinate (hi relative to the
+// item's centre, and its FP32 low part).
+struct TargetPair {
+  float2 x, y, z, lx, ly, lz;
+};
+
+// Target against a source pair. n* are the NEGATED source coordinates (hi and,
+// for NEAR, lo). NEAR forms the difference as (t_hi - s_hi) + (t_lo - s_lo), so
+// near-field pairs (touching PP sources) keep their separation to ~1e-14
+// relative to the centre distance, not FP32's 6e-8.
 template <int DIM, int KIND, bool NEAR>
-__device__ __forceinline__ void eval_fp32(float tx, float ty, float tz, float lx, float ly, float lz, const float4& s,
-                                          const float4& sl, float eps2, float* acc) {
-  const float dx = NEAR ? (tx - s.x) + (lx - sl.x) : tx - s.x;
-  const float dy = NEAR ? (ty - s.y) + (ly - sl.y) : ty - s.y;
+__device__ __forceinline__ void eval_pair(const TargetPair& t, float2 nx, float2 ny, float2 nz, float2 w, float2 nlx,
+                                          float2 nly, float2 nlz, float2 e2, float2* acc) {
+  float2 dx = add2(t.x, nx), dy = add2(t.y, ny);
+  if (NEAR) {
+    dx = add2(dx, add2(t.lx, nlx));
+    dy = add2(dy, add2(t.ly, nly));
+  }
   if (DIM == 2) {
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, eps2));
-    acc[0] = fmaf(s.w, __logf(r2), acc[0]);
+    const float2 r2 = fma2(dx, dx, fma2(dy, dy, e2));
+    acc[0] = fma2(w, make_float2(__logf(r2.x), __logf(r2.y)), acc[0]);
     if (KIND == BTK_KIND_FIELD) {
-      const float g = s.w * rcp_fp32(r2);
-      acc[1] = fmaf(dx, g, acc[1]);
-      acc[2] = fmaf(dy, g, acc[2]);
+      const float2 g = mul2(w, make_float2(rcp_fp32(r2.x), rcp_fp32(r2.y)));
+      acc[1] = fma2(dx, g, acc[1]);
+      acc[2] = fma2(dy, g, acc[2]);
     }
   } else {
-    const float dz = NEAR ? (tz - s.z) + (lz - sl.z) : tz - s.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+    float2 dz = add2(t.z, nz);
+    if (NEAR) dz = add2(dz, add2(t.lz, nlz));
+    const float2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, e2)));
     if (KIND == BTK_KIND_VEL) {
-      const float g = s.w * rcp_fp32(r2);
-      acc[0] = fmaf(dx, g, acc[0]);
-      acc[1] = fmaf(dy, g, acc[1]);
-      acc[2] = fmaf(dz, g, acc[2]);
+      const float2 g = mul2(w, make_float2(rcp_fp32(r2.x), rcp_fp32(r2.y)));
+      acc[0] = fma2(dx, g, acc[0]);
+      acc[1] = fma2(dy, g, acc[1]);
+      acc[2] = fma2(dz, g, acc[2]);
     } else {
-      const float ri = rsqrt_fp32(r2);
+      const float2 ri = make_float2(rsqrt_fp32(r2.x), rsqrt_fp32(r2.y));
       if (KIND == BTK_KIND_POT) {
-        acc[0] = fmaf(s.w, ri, acc[0]);
+        acc[0] = fma2(w, ri, acc[0]);
       } else {
-        const float wr = s.w * ri;
-        acc[0] += wr;
-        const float g = wr * (ri * ri);
-        acc[1] = fmaf(dx, g, acc[1]);
-        acc[2] = fmaf(dy, g, acc[2]);
-        acc[3] = fmaf(dz, g, acc[3]);
+        const float2 wr = mul2(w, ri);
+        acc[0] = add2(acc[0], wr);
+        const float2 g = mul2(wr, mul2(ri, ri));
+        acc[1] = fma2(dx, g, acc[1]);
+        acc[2] = fma2(dy, g, acc[2]);
+        acc[3] = fma2(dz, g, acc[3]);
       }
     }
+  }
+}
+
+// Source pairs [j0, j1) of a converted chunk against NU targets.
+template <int DIM, int KIND, bool NEAR, int NU, int NC>
+__device__ __forceinline__ void pair_loop(const float4* fA, const float4* fB, const float4* fL, const float2* fLz,
+                                          int j0, int j1, const TargetPair* T, float2 e2, float2 (*part)[NC]) {
+#pragma unroll 2
+  for (int j = j0; j < j1; ++j) {
+    const float4 a = fA[j], b = fB[j];
+    float4 l = make_float4(0.f, 0.f, 0.f, 0.f);
+    float2 lz = make_float2(0.f, 0.f);
+    if (NEAR) {
+      l = fL[j];
+      lz = fLz[j];
+    }
+#pragma unroll
+    for (int u = 0; u < NU; ++u)
+      eval_pair<DIM, KIND, NEAR>(T[u], make_float2(a.x, a.y), make_float2(a.z, a.w), make_float2(b.x, b.y),
+                                 make_float2(b.z, b.w), make_float2(l.x, l.y), make_float2(l.z, l.w), lz, e2, part[u]);
   }
 }
 
@@ -262,23 +318,30 @@ __device__ __forceinline__ void two_sum_add(double& sum, double& comp, double b)
 }
 
 template <int DIM, int KIND>
-__global__ void __launch_bounds__(kInteractThreads, 6) k_interact_mixed(InteractParams p) {
+__global__ void __launch_bounds__(kInteractThreads, 4) k_interact_mixed(InteractParams p) {
   constexpr int NC = KernelTraits<DIM, KIND>::NC;
   constexpr int TPT = kTargetsPerThread;
+  static_assert(TPT == 2, "targets of a warp are [64 w, 64 w + 64): two per thread");
   __shared__ __align__(128) double4 sbuf[kStages][kChunk];
-  __shared__ __align__(16) float4 fbuf[kChunk], fbuf_lo[kChunk];
+  // converted chunk, by source pair j = (2j, 2j+1): negated hi coordinates and
+  // weights, negated lo coordinates
+  // (double-buffered: chunk c is converted into buffer c & 1 while other warps
+  // may still evaluate chunk c - 1 from the other buffer)
+  __shared__ __align__(16) float4 fA[2][kPairs], fB[2][kPairs], fL[2][kPairs];
+  __shared__ __align__(16) float2 fLz[2][kPairs];
   __shared__ __align__(8) uint64_t bars[kStages];
   __shared__ int s_item, s_abort;
   __shared__ uint32_t s_fail_chunk;
 
   const int tid = threadIdx.x;
+  const int lane = tid & 31, tbase = (tid >> 5) * 64;
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
     s_abort = 0;
   }
   __syncthreads();
-  const float eps2 = (float)p.eps2;
+  const float2 e2 = make_float2((float)p.eps2, (float)p.eps2);
 
   uint32_t g = 0;
   int pe = 0, poff = 0;
@@ -318,15 +381,26 @@ __global__ void __launch_bounds__(kInteractThreads, 6) k_interact_mixed(Interact
       for (int c = 0; c < min(kStages, n_chunks); ++c) issue(c);
     }
 
-    float tx[TPT], ty[TPT], tz[TPT], lx[TPT], ly[TPT], lz[TPT];
+    // This warp's targets: [tbase, tbase + 64) of the tile, nu of its two
+    // 32-target halves in use (warp-uniform), so a partly filled tile leaves
+    // its idle warps' issue slots to other blocks.
+    const int nu = w.t_count > tbase + 32 ? 2 : (w.t_count > tbase ? 1 : 0);
+    TargetPair T[TPT];
     double acc[TPT][NC], comp[TPT][NC];
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int i = min(tid + u * kInteractThreads, w.t_count - 1);
-      const double4 t = p.T4[w.t_begin + i];
-      split_rel(t.x, w.cx, tx[u], lx[u]);
-      split_rel(t.y, w.cy, ty[u], ly[u]);
-      split_rel(t.z, w.cz, tz[u], lz[u]);
+      const int i = min(tbase + u * 32 + lane, w.t_count - 1);
+      const double4 t = ((w.flags & kItemAudit) ? p.T4a : p.T4)[w.t_begin + i];
+      float h, l;
+      split_rel(t.x, w.cx, h, l);
+      T[u].x = make_float2(h, h);
+      T[u].lx = make_float2(l, l);
+      split_rel(t.y, w.cy, h, l);
+      T[u].y = make_float2(h, h);
+      T[u].ly = make_float2(l, l);
+      split_rel(t.z, w.cz, h, l);
+      T[u].z = make_float2(h, h);
+      T[u].lz = make_float2(l, l);
 #pragma unroll
       for (int c = 0; c < NC; ++c) acc[u][c] = comp[u][c] = 0.0;
     }
@@ -339,64 +413,79 @@ __global__ void __launch_bounds__(kInteractThreads, 6) k_interact_mixed(Interact
         s_fail_chunk = g + c;
         atomicCAS(p.status, 0, (int)BTK_ERR_DEVICE_TIMEOUT);
       }
-      __syncthreads();
-      if (s_abort) break;
       const int cnt = min(kChunk, w.s_total - c * kChunk);
       const int near_end = min(cnt, max(0, w.near_total - c * kChunk));  // near sources of this chunk
-      for (int j = tid; j < cnt; j += kInteractThreads) {
-        const double4 s = sbuf[stage][j];
-        float4 h, l;
-        split_rel(s.x, w.cx, h.x, l.x);
-        split_rel(s.y, w.cy, h.y, l.y);
-        split_rel(s.z, w.cz, h.z, l.z);
-        h.w = (float)s.w;
-        l.w = 0.f;
-        fbuf[j] = h;
-        fbuf_lo[j] = l;
+      const int b = c & 1;
+      {  // thread tid converts source pair tid into buffer b
+        float hx[2], hy[2], hz[2], lx[2], ly[2], lz[2], ww[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int j = 2 * tid + k;
+          if (j < cnt) {
+            const double4 s = sbuf[stage][j];
+            split_rel(s.x, w.cx, hx[k], lx[k]);
+            split_rel(s.y, w.cy, hy[k], ly[k]);
+            split_rel(s.z, w.cz, hz[k], lz[k]);
+            hx[k] = -hx[k];
+            hy[k] = -hy[k];
+            hz[k] = -hz[k];
+            lx[k] = -lx[k];
+            ly[k] = -ly[k];
+            lz[k] = -lz[k];
+            ww[k] = (float)s.w;
+          } else {
+            hx[k] = hy[k] = hz[k] = kPadCoord;
+            lx[k] = ly[k] = lz[k] = 0.f;
+            ww[k] = 0.f;
+          }
+        }
+        fA[b][tid] = make_float4(hx[0], hx[1], hy[0], hy[1]);
+        fB[b][tid] = make_float4(hz[0], hz[1], ww[0], ww[1]);
+        fL[b][tid] = make_float4(lx[0], lx[1], ly[0], ly[1]);
+        fLz[b][tid] = make_float2(lz[0], lz[1]);
       }
+      // One barrier per chunk: buffer b is complete, every thread has finished
+      // chunk c - 1 (so buffer b ^ 1 may be overwritten next), and the FP64
+      // stage has been read, so it is refilled while this chunk is evaluated.
       __syncthreads();
-      // The FP64 stage is free again: refill it while this chunk is evaluated.
+      if (s_abort) break;
       if (tid == 0 && c + kStages < n_chunks) issue(c + kStages);
-      for (int f0 = 0; f0 < cnt; f0 += kFold) {
-        const int f1 = min(cnt, f0 + kFold);
-        float part[TPT][NC];
+      const int np = (cnt + 1) / 2, nnp = (near_end + 1) / 2;  // a pair with one near source is near
+      for (int f0 = 0; f0 < np; f0 += kFoldPairs) {
+        const int f1 = min(np, f0 + kFoldPairs);
+        const int fn = min(f1, max(f0, nnp));
+        float2 part[TPT][NC];
 #pragma unroll
         for (int u = 0; u < TPT; ++u)
 #pragma unroll
-          for (int k = 0; k < NC; ++k) part[u][k] = 0.f;
-        const int fn = min(f1, max(f0, near_end));
-#pragma unroll 2
-        for (int j = f0; j < fn; ++j) {
-          const float4 s = fbuf[j], sl = fbuf_lo[j];
-#pragma unroll
-          for (int u = 0; u < TPT; ++u)
-            eval_fp32<DIM, KIND, true>(tx[u], ty[u], tz[u], lx[u], ly[u], lz[u], s, sl, eps2, part[u]);
-        }
-#pragma unroll 4
-        for (int j = fn; j < f1; ++j) {
-          const float4 s = fbuf[j];
-#pragma unroll
-          for (int u = 0; u < TPT; ++u)
-            eval_fp32<DIM, KIND, false>(tx[u], ty[u], tz[u], lx[u], ly[u], lz[u], s, s, eps2, part[u]);
+          for (int k = 0; k < NC; ++k) part[u][k] = make_float2(0.f, 0.f);
+        if (nu == 2) {
+          pair_loop<DIM, KIND, true, 2, NC>(fA[b], fB[b], fL[b], fLz[b], f0, fn, T, e2, part);
+          pair_loop<DIM, KIND, false, 2, NC>(fA[b], fB[b], fL[b], fLz[b], fn, f1, T, e2, part);
+        } else if (nu == 1) {
+          pair_loop<DIM, KIND, true, 1, NC>(fA[b], fB[b], fL[b], fLz[b], f0, fn, T, e2, part);
+          pair_loop<DIM, KIND, false, 1, NC>(fA[b], fB[b], fL[b], fLz[b], fn, f1, T, e2, part);
         }
 #pragma unroll
         for (int u = 0; u < TPT; ++u)
+          if (u < nu) {
 #pragma unroll
-          for (int k = 0; k < NC; ++k) two_sum_add(acc[u][k], comp[u][k], (double)part[u][k]);
+            for (int k = 0; k < NC; ++k) two_sum_add(acc[u][k], comp[u][k], (double)(part[u][k].x + part[u][k].y));
+          }
       }
-      __syncthreads();
     }
     if (s_abort) break;
     g += n_chunks;
 
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int i = tid + u * kInteractThreads;
+      const int i = tbase + u * 32 + lane;
       if (i < w.t_count) {
-        const int idx = p.T_out[w.t_begin + i];
+        const bool audit = (w.flags & kItemAudit) != 0;
+        const int idx = audit ? w.t_begin + i : p.T_out[w.t_begin + i];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          double* dst = ((w.flags & kItemProxyTargets) ? p.ptw[c] : p.out[c]) + idx;
+          double* dst = (audit ? p.aout[c] : (w.flags & kItemProxyTargets) ? p.ptw[c] : p.out[c]) + idx;
           const double v = (acc[u][c] + comp[u][c]) * p.scale[c];
           if (w.flags & kItemAtomic)
             atomicAdd(dst, v);

@@ -133,7 +133,12 @@ btk_status side_layout(Side& S, int n_points, int degree) {
                   "tree: inconsistent child/parent links");
       }
     }
-    if (i > 0) BTK_CHECK(h.parent[i] >= 0 && h.parent[i] < i, BTK_ERR_INVALID_ARGUMENT, "tree: bad parent link");
+    // Level-0 panels are roots (one per tree: a forest of independent trees,
+    // as a batch builds, has several); every other panel's parent precedes it.
+    if (h.level[i] > 0)
+      BTK_CHECK(h.parent[i] >= 0 && h.parent[i] < i, BTK_ERR_INVALID_ARGUMENT, "tree: bad parent link");
+    else
+      BTK_CHECK(h.parent[i] == -1, BTK_ERR_INVALID_ARGUMENT, "tree: a level-0 panel with a parent");
   }
   return BTK_OK;
 }
@@ -223,9 +228,11 @@ struct WorkLists {
 // pc_begin (optional): S4 start of each PC pair's source proxies (default: the
 // cluster's single-degree slot). pc_entry (optional, out): final entry index of
 // each PC pair, for re-pointing when per-pair degrees change.
+// split: work items per persistent-grid slot the cost cap aims at (longer
+// source lists are cut into atomic pieces).
 btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* const lists[4], const int counts[4],
                       int grid_slots, WorkLists& W, const std::vector<long long>* pc_begin = nullptr,
-                      std::vector<int>* pc_entry = nullptr) {
+                      std::vector<int>* pc_entry = nullptr, int split = 8) {
   const int ipc = S.ipc;
   const int nt = T.n_points, ns = S.n_points;
   const int Pt = T.h.panel_count, Ps = S.h.panel_count;
@@ -288,7 +295,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
   // Tiles and items.
   int64_t total_cost = W.evals[0] + W.evals[1] + W.evals[2] + W.evals[3];
   const int64_t max_cost =
-      std::max<int64_t>((int64_t)kTile * 8192, total_cost / std::max<int64_t>(1, (int64_t)grid_slots * 8));
+      std::max<int64_t>((int64_t)kTile * 8192, total_cost / std::max<int64_t>(1, (int64_t)grid_slots * split));
   std::vector<std::pair<int64_t, WorkItem>> items;
   for (int tp = 0; tp < Pt; ++tp) {
     const int eb = head[tp], ee = head[tp + 1];
@@ -392,6 +399,8 @@ struct InteractCtx {
   Entry* d_entries = nullptr;
   int n_items = 0;
   int* d_ticket_status = nullptr;  // [0] ticket, [1] status
+  const double4* d_T4a = nullptr;  // audit targets and outputs (kItemAudit items)
+  Ptr4 aout{};
 };
 
 btk_status run_interactions(const InteractCtx& C, const double4* S4, const double4* T4, const int* T_out,
@@ -407,7 +416,9 @@ btk_status run_interactions(const InteractCtx& C, const double4* S4, const doubl
   for (int c = 0; c < 4; ++c) {
     p.out[c] = out.p[c];
     p.ptw[c] = ptw.p[c];
+    p.aout[c] = C.aout.p[c];
   }
+  p.T4a = C.d_T4a;
   p.eps2 = C.eps * C.eps;
   kind_scales(C.dim, C.kind, p.scale);
   p.ticket = C.d_ticket_status;
@@ -512,15 +523,16 @@ struct btk_plan {
   int *d_pc_tcount = nullptr, *d_cp_scount = nullptr;
   float *d_desc = nullptr, *d_feat = nullptr, *d_pred = nullptr;
   unsigned long long* d_evals = nullptr;
-  int* d_hist = nullptr;
   double* d_gsum = nullptr;  // sum |q|, sum q
   double root_radius = 1.0, root_centre[3] = {0, 0, 0};
-  // audit: a fixed 1% sample of the targets, direct sum over all sources
-  int n_audit = 0;
-  int *d_audit_orig = nullptr, *d_audit_tout = nullptr;
+  // audit: a fixed 1% sample of the targets, direct sum over all sources; its
+  // work items follow the solve's in ictx.d_items, [n_items_main, + n_audit_items)
+  int n_audit = 0, n_items_main = 0, n_audit_items = 0;
+  int work_split = 8;  // work items per persistent-grid slot
+  int* d_audit_orig = nullptr;
   double4* d_audit_T4 = nullptr;
   double *d_audit_out = nullptr, *d_audit_sums = nullptr;
-  btk::InteractCtx audit_ctx;
+  int* d_report = nullptr;  // degree histogram (kMaxNodes ints), copied with the audit sums
   int *d_cluster_slot_s = nullptr, *d_cluster_slot_t = nullptr;  // panel -> cluster index (or -1)
 };
 
@@ -563,6 +575,9 @@ void recount_far_evals(btk_plan* P) {
   for (int i = 0; i < P->n_cp; ++i) P->evals[2] += sz(P->h_deg_far[i]) * P->h_cp_scount[i];
   for (int i = P->n_cp; i < P->n_far; ++i) P->evals[3] += sz(P->h_deg_far[i]) * sz(P->h_deg_far[i]);
 }
+
+void audit_layout(int nt, int ns, int* na, int* tiles, int* pieces);
+btk_status setup_audit(btk_plan* P, Arena& A, int item_base, int entry_base, cudaStream_t st);
 
 btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists[4], const int counts[4], int slots,
                                cudaStream_t st) {
@@ -649,7 +664,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   const int counts_static[4] = {counts[0], counts[1], 0, 0};
   WorkLists W;
   std::vector<int> pc_entry;
-  BTK_TRY(build_work(T, S, lists, counts_static, slots, W, &pc_begin, &pc_entry));
+  BTK_TRY(build_work(T, S, lists, counts_static, slots, W, &pc_begin, &pc_entry, P->work_split));
   P->evals[0] = W.evals[0];
   P->n_static_items = (int)W.items.size();
   P->n_static_entries = (int)W.entries.size();
@@ -690,9 +705,13 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   BTK_TRY(A.upload(&P->d_far_src, far_src));
   BTK_TRY(A.upload(&P->d_tgt_centre, centre));
   const size_t n_items = (size_t)P->n_static_items + (size_t)P->n_far * P->tiles_max;
-  BTK_CHECK(n_items < (1u << 31), BTK_ERR_UNSUPPORTED, "too many work items");
-  BTK_TRY(A.alloc(&P->ictx.d_items, std::max<size_t>(n_items, 1)));
-  BTK_TRY(A.alloc(&P->ictx.d_entries, std::max<size_t>((size_t)P->n_static_entries + P->n_far, 1)));
+  int a_na, a_tiles, a_pieces;
+  audit_layout(T.n_points, S.n_points, &a_na, &a_tiles, &a_pieces);
+  const size_t n_audit_items = (size_t)a_tiles * a_pieces;
+  BTK_CHECK(n_items + n_audit_items < (1u << 31), BTK_ERR_UNSUPPORTED, "too many work items");
+  // items: [static PP/PC | far CP/CC tiles | audit]; entries: [static | far | audit]
+  BTK_TRY(A.alloc(&P->ictx.d_items, std::max<size_t>(n_items + n_audit_items, 1)));
+  BTK_TRY(A.alloc(&P->ictx.d_entries, std::max<size_t>((size_t)P->n_static_entries + P->n_far + a_pieces, 1)));
   if (!W.items.empty())
     BTK_CUDA(cudaMemcpyAsync(P->ictx.d_items, W.items.data(), sizeof(WorkItem) * W.items.size(),
                              cudaMemcpyHostToDevice, st));
@@ -700,6 +719,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     BTK_CUDA(cudaMemcpyAsync(P->ictx.d_entries, W.entries.data(), sizeof(Entry) * W.entries.size(),
                              cudaMemcpyHostToDevice, st));
   P->ictx.n_items = (int)n_items;
+  P->n_items_main = (int)n_items;
   // Degrees in force: all at n until set.
   P->h_deg_pc.assign(P->n_pc, n);
   P->h_deg_far.assign(P->n_far, n);
@@ -737,7 +757,6 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     BTK_TRY(A.alloc(&P->d_feat, (size_t)std::max(P->n_pairs, 1) * 16));
     BTK_TRY(A.alloc(&P->d_pred, (size_t)std::max(P->n_pairs, 1) * 9));
     BTK_TRY(A.alloc(&P->d_evals, 1));
-    BTK_TRY(A.alloc(&P->d_hist, kMaxNodes));
     BTK_TRY(A.alloc(&P->d_gsum, 2));
     BTK_TRY(A.upload(&P->d_cluster_slot_s, S.cluster_slot));
     BTK_TRY(A.upload(&P->d_cluster_slot_t, T.cluster_slot));
@@ -749,6 +768,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     }
     P->root_radius = std::max(0.5 * std::sqrt(r2), 1e-300);
   }
+  BTK_TRY(setup_audit(P, A, P->n_items_main, P->n_static_entries + P->n_far, st));
   // Work arrays.
   BTK_TRY(A.alloc(&P->d_S4, (size_t)S.n_points + P->total_src_slots + 1));
   BTK_TRY(A.alloc(&P->d_T4, (size_t)T.n_points + P->total_tgt_slots + 1));
@@ -772,8 +792,10 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
   BTK_CHECK(!(D->kind == BTK_KIND_VEL && cfg.dim != 3), BTK_ERR_UNSUPPORTED, "VEL kernel is 3-D only");
   BTK_CHECK(D->precision == BTK_PREC_FP64 || D->precision == BTK_PREC_MIXED, BTK_ERR_UNSUPPORTED,
             "precision must be BTK_PREC_FP64 or BTK_PREC_MIXED");
-  BTK_CHECK(D->tree_target && D->panels_target && D->panel_points_inside_target && D->point_leaf_panel_source,
-            BTK_ERR_INVALID_ARGUMENT, "plan: missing tree arrays");
+  BTK_CHECK(D->tree_target && D->panels_target && D->point_leaf_panel_source, BTK_ERR_INVALID_ARGUMENT,
+            "plan: missing tree arrays");
+  BTK_CHECK(D->panel_points_inside_target || D->panels_source == nullptr, BTK_ERR_INVALID_ARGUMENT,
+            "plan: panel_points_inside_target may be NULL only with one tree (leaf order from point_leaf_panel)");
   P->dim = cfg.dim;
   P->degree = cfg.interp_degree;
   P->m = P->degree + 1;
@@ -792,6 +814,9 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
                         D->tree_target->levels, P->tgt.h);
   BTK_TRY(side_layout(P->tgt, D->point_count_target, P->degree));
   BTK_TRY(side_upload(P->tgt, A, D->panel_points_inside_target, nullptr, P->thresh));
+  if (!D->panel_points_inside_target)
+    BTK_TRY(side_perm_from_leaf_of(P->tgt, A, std::vector<int>(D->point_leaf_panel_source,
+                                                               D->point_leaf_panel_source + D->point_count_target)));
   if (P->same_tree) {
     P->src = &P->tgt;
     BTK_CHECK(D->point_count_source == D->point_count_target, BTK_ERR_INVALID_ARGUMENT,
@@ -827,12 +852,14 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
   BTK_TRY(A.alloc(&P->d_ptw, (size_t)P->ncomp * Pt * P->ipc));
   P->degree_mode = D->degree_mode;
   P->degree_min = D->degree_min;
+  BTK_CHECK(D->work_split >= 0 && D->work_split <= 1024, BTK_ERR_INVALID_ARGUMENT, "work_split outside 0..1024");
+  P->work_split = D->work_split > 0 ? D->work_split : 8;
   BTK_CHECK(D->degree_mode == BTK_DEGREE_FIXED || D->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT,
             "bad degree_mode");
 
   if (D->degree_mode == BTK_DEGREE_FIXED) {
     WorkLists W;
-    BTK_TRY(build_work(T, S, lists, counts, slots, W));
+    BTK_TRY(build_work(T, S, lists, counts, slots, W, nullptr, nullptr, P->work_split));
     for (int t = 0; t < 4; ++t) P->evals[t] = W.evals[t];
     P->ictx.n_items = (int)W.items.size();
     BTK_TRY(A.upload(&P->ictx.d_items, W.items));
@@ -977,12 +1004,23 @@ namespace {
 // A fixed, seeded 1% sample of the targets (at least one), and work items for
 // the direct sum over every source: tiles of kTile audited targets times
 // pieces of the sorted source points, all sources on the hi/lo path.
-btk_status setup_audit(btk_plan* P, cudaStream_t st) {
-  if (P->n_audit > 0) return BTK_OK;
-  Arena& A = *P->arena;
+// Audit layout: na targets (one per 100, at least one when there are
+// targets), kTile targets per tile, the sources cut into pieces of
+// kAuditPiece so the items are small tail-fillers of the solve's launch.
+constexpr int kAuditPiece = 4096;
+void audit_layout(int nt, int ns, int* na, int* tiles, int* pieces) {
+  *na = nt > 0 ? std::max(1, nt / 100) : 0;
+  *tiles = (*na + kTile - 1) / kTile;
+  *pieces = ns > 0 ? (ns + kAuditPiece - 1) / kAuditPiece : 0;
+}
+
+// Builds the audit sample and its work items into ictx's arrays at
+// item_base / entry_base (capacity reserved by the caller).
+btk_status setup_audit(btk_plan* P, Arena& A, int item_base, int entry_base, cudaStream_t st) {
   const int nt = P->tgt.n_points, ns = P->src->n_points;
-  const int na = std::max(1, nt / 100);
-  std::vector<int> orig(na);
+  int na, tiles, pieces;
+  audit_layout(nt, ns, &na, &tiles, &pieces);
+  std::vector<int> orig(std::max(na, 1), 0);
   // Evenly spread, seeded offsets (SplitMix64-style hash) over the index range.
   for (int k = 0; k < na; ++k) {
     uint64_t z = 0x9E3779B97F4A7C15ULL * (uint64_t)(k + 1);
@@ -992,44 +1030,41 @@ btk_status setup_audit(btk_plan* P, cudaStream_t st) {
     const int64_t lo = (int64_t)k * nt / na, hi = (int64_t)(k + 1) * nt / na;
     orig[k] = (int)(lo + (int64_t)(z % (uint64_t)std::max<int64_t>(1, hi - lo)));
   }
-  std::vector<int> tout(na);
-  std::iota(tout.begin(), tout.end(), 0);
   BTK_TRY(A.upload(&P->d_audit_orig, orig));
-  BTK_TRY(A.upload(&P->d_audit_tout, tout));
-  BTK_TRY(A.alloc(&P->d_audit_T4, (size_t)na));
-  BTK_TRY(A.alloc(&P->d_audit_out, (size_t)P->ncomp * na));
+  BTK_TRY(A.alloc(&P->d_audit_T4, (size_t)std::max(na, 1)));
+  BTK_TRY(A.alloc(&P->d_audit_out, (size_t)P->ncomp * std::max(na, 1)));
   BTK_TRY(A.alloc(&P->d_audit_sums, 2));
-  const int tiles = (na + kTile - 1) / kTile;
-  const int slots = num_sms() * 6;
-  const int pieces = std::max(1, std::min(ns, (2 * slots + tiles - 1) / tiles));
+  BTK_TRY(A.alloc(&P->d_report, kMaxNodes));
   std::vector<Entry> entries;
   std::vector<WorkItem> items;
   for (int p = 0; p < pieces; ++p) {
-    const int b = (int)((int64_t)p * ns / pieces), e = (int)((int64_t)(p + 1) * ns / pieces);
-    if (e > b) entries.push_back(Entry{b, e - b});
+    const int b = p * kAuditPiece, e = std::min(ns, b + kAuditPiece);
+    entries.push_back(Entry{b, e - b});
   }
   for (int t = 0; t < tiles; ++t)
-    for (int p = 0; p < (int)entries.size(); ++p) {
+    for (int p = 0; p < pieces; ++p) {
       WorkItem w{};
       w.t_begin = t * kTile;
       w.t_count = std::min(kTile, na - t * kTile);
-      w.e_begin = p;
-      w.e_end = p + 1;
+      w.e_begin = entry_base + p;
+      w.e_end = entry_base + p + 1;
       w.s_total = entries[p].s_count;
-      w.flags = kItemAtomic;
-      w.near_total = w.s_total;
+      w.flags = kItemAtomic | kItemAudit;
+      w.near_total = w.s_total;  // every source takes the hi/lo path
       w.cx = P->root_centre[0];
       w.cy = P->root_centre[1];
       w.cz = P->root_centre[2];
       items.push_back(w);
     }
-  P->audit_ctx = P->ictx;
-  P->audit_ctx.n_items = (int)items.size();
-  BTK_TRY(A.upload(&P->audit_ctx.d_items, items));
-  BTK_TRY(A.upload(&P->audit_ctx.d_entries, entries));
-  BTK_TRY(A.alloc(&P->audit_ctx.d_ticket_status, 2));
-  BTK_CUDA(cudaMemsetAsync(P->audit_ctx.d_ticket_status, 0, 2 * sizeof(int), st));
+  if (!items.empty()) {
+    BTK_CUDA(cudaMemcpyAsync(P->ictx.d_items + item_base, items.data(), sizeof(WorkItem) * items.size(),
+                             cudaMemcpyHostToDevice, st));
+    BTK_CUDA(cudaMemcpyAsync(P->ictx.d_entries + entry_base, entries.data(), sizeof(Entry) * entries.size(),
+                             cudaMemcpyHostToDevice, st));
+    BTK_CUDA(cudaStreamSynchronize(st));  // the host vectors go out of scope
+  }
   P->n_audit = na;
+  P->n_audit_items = (int)items.size();
   return BTK_OK;
 }
 
@@ -1107,7 +1142,6 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   Side& T = P->tgt;
   Side& S = *P->src;
   const int Pt = T.h.panel_count;
-  BTK_TRY(setup_audit(P, st));
   cudaEvent_t e[4];
   for (auto& x : e) BTK_CUDA(cudaEventCreate(&x));
   BTK_CUDA(cudaEventRecord(e[0], st));
@@ -1117,9 +1151,9 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   const int lo = std::max(std::max(degree_lo, P->degree_min), 1);
   BTK_CUDA(launch_choose_degrees(P->n_pairs, P->d_pred, (float)std::log10(pair_tol), lo, P->degree, P->d_deg_pc, st));
   BTK_CUDA(cudaMemsetAsync(P->d_evals, 0, sizeof(unsigned long long), st));
-  BTK_CUDA(cudaMemsetAsync(P->d_hist, 0, sizeof(int) * kMaxNodes, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_report, 0, sizeof(int) * kMaxNodes, st));
   BTK_CUDA(launch_far_evals(P->dim, P->n_pc, P->n_cp, P->n_far - P->n_cp, P->d_deg_pc, P->d_pc_tcount,
-                            P->d_cp_scount, P->d_evals, st));
+                            P->d_cp_scount, P->d_evals, P->d_report, st));
   BTK_CUDA(cudaEventRecord(e[1], st));
   // Solve at the chosen degrees.
   Ptr4 o{}, w{}, wm{};
@@ -1155,30 +1189,27 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     BTK_TRY(run_downward(T, P->ncomp, P->d_T4, w, o, st));
     return BTK_OK;
   };
-  BTK_TRY(solve(P->ictx));
-  BTK_CUDA(cudaEventRecord(e[2], st));
-  // Audit: direct sum at the sampled targets.
+  // The audit (direct sum at the sampled targets) runs as the last work items
+  // of the solve's own launch, filling its tail.
   BTK_CUDA(launch_gather(P->n_audit, P->d_audit_orig, xt, yt, P->dim == 3 ? zt : nullptr, nullptr, P->d_audit_T4, st));
-  BTK_CUDA(cudaMemsetAsync(P->d_audit_out, 0, sizeof(double) * (size_t)P->ncomp * P->n_audit, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_audit_out, 0, sizeof(double) * (size_t)P->ncomp * std::max(P->n_audit, 1), st));
   BTK_CUDA(cudaMemsetAsync(P->d_audit_sums, 0, 2 * sizeof(double), st));
-  Ptr4 ao{};
-  for (int c = 0; c < P->ncomp; ++c) ao.p[c] = P->d_audit_out + (size_t)c * P->n_audit;
-  BTK_TRY(run_interactions(P->audit_ctx, P->d_S4, P->d_audit_T4, P->d_audit_tout, ao, ao, st));
+  InteractCtx with_audit = P->ictx;
+  with_audit.n_items = P->n_items_main + P->n_audit_items;
+  with_audit.d_T4a = P->d_audit_T4;
+  for (int c = 0; c < P->ncomp; ++c) with_audit.aout.p[c] = P->d_audit_out + (size_t)c * P->n_audit;
+  BTK_TRY(solve(with_audit));
+  BTK_CUDA(cudaEventRecord(e[2], st));
   BTK_CUDA(launch_audit_compare(P->n_audit, P->ncomp, T.n_points, P->d_audit_orig, nullptr, out, P->d_audit_out,
                                 P->d_audit_sums, st));
   double sums[2] = {0, 0};
   unsigned long long ev = 0;
+  int hist[kMaxNodes] = {0};  // degrees the selector chose (before any fallback)
   BTK_CUDA(cudaMemcpyAsync(sums, P->d_audit_sums, sizeof(sums), cudaMemcpyDeviceToHost, st));
   BTK_CUDA(cudaMemcpyAsync(&ev, P->d_evals, sizeof(ev), cudaMemcpyDeviceToHost, st));
+  BTK_CUDA(cudaMemcpyAsync(hist, P->d_report, sizeof(hist), cudaMemcpyDeviceToHost, st));
   BTK_CUDA(cudaStreamSynchronize(st));
   const double rel = std::sqrt(sums[0] / std::max(sums[1], 1e-300));
-  int hist[13] = {0};
-  if (report && P->n_pairs) {  // degrees the selector chose (before any fallback)
-    std::vector<int> deg(P->n_pairs);
-    BTK_CUDA(cudaMemcpy(deg.data(), P->d_deg_pc, sizeof(int) * P->n_pairs, cudaMemcpyDeviceToHost));
-    for (int d : deg)
-      if (d >= 0 && d < 13) hist[d]++;
-  }
   int fell_back = 0;
   if (!(rel <= tol)) {
     // Fallback: the fixed-degree plain method (degree n everywhere, FP64).

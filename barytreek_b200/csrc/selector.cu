@@ -328,10 +328,14 @@ __global__ void k_choose_degrees(int n, const float* pred, float log10_target, i
 
 // Far-field evaluations at the chosen degrees (pairs PC, CP, CC in order).
 __global__ void k_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
-                            const int* cp_scount, unsigned long long* evals) {
+                            const int* cp_scount, unsigned long long* evals, int* hist) {
+  __shared__ int sh[kMaxDegree + 1];
+  if (threadIdx.x <= kMaxDegree) sh[threadIdx.x] = 0;
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long v = 0;
   const int n = n_pc + n_cp + n_cc;
+  if (i < n && deg[i] >= 0 && deg[i] <= kMaxDegree) atomicAdd(&sh[deg[i]], 1);
   if (i < n) {
     const unsigned long long m = (unsigned long long)(deg[i] + 1);
     const unsigned long long s = dim == 3 ? m * m * m : m * m;
@@ -344,6 +348,8 @@ __global__ void k_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* de
   }
   for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(evals, v);
+  __syncthreads();
+  if (threadIdx.x <= kMaxDegree && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
 }
 
 // Audit: sums of |treecode - direct|^2 and |direct|^2 over the audited
@@ -559,10 +565,10 @@ __global__ void k_fill_int(int n, int value, int* dst) {
 int selector_param_count() { return kParams; }
 
 cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
-                             const int* cp_scount, unsigned long long* evals, cudaStream_t s) {
+                             const int* cp_scount, unsigned long long* evals, int* hist, cudaStream_t s) {
   const int n = n_pc + n_cp + n_cc;
   if (n <= 0) return cudaSuccess;
-  k_far_evals<<<(n + 255) / 256, 256, 0, s>>>(dim, n_pc, n_cp, n_cc, deg, pc_tcount, cp_scount, evals);
+  k_far_evals<<<(n + 255) / 256, 256, 0, s>>>(dim, n_pc, n_cp, n_cc, deg, pc_tcount, cp_scount, evals, hist);
   count_launch();
   return cudaGetLastError();
 }

@@ -143,12 +143,13 @@ class Treecode:
     """
 
     def __init__(self, coords, sources=None, *, degree=8, cluster_size=100, theta=0.7, eps=1e-4, kind=KIND_POT,
-                 precision=PREC_FP64, degree_mode=_lib.DEGREE_FIXED, degree_min=1, device="cuda"):
+                 precision=PREC_FP64, degree_mode=_lib.DEGREE_FIXED, degree_min=1, work_split=0, device="cuda"):
         import torch
 
         self.dim = len(coords)
         self.kind, self.precision = kind, precision
         self.degree_mode, self.degree_min = degree_mode, degree_min
+        self.work_split = work_split
         self.ncomp = ncomp(self.dim, kind)
         self.cfg = make_run_config(self.dim, degree, cluster_size, theta, eps)
         self.targets = tuple(np.ascontiguousarray(c, np.float64) for c in coords)
@@ -186,6 +187,7 @@ class Treecode:
         d.pp_list, d.pc_list, d.cp_list, d.cc_list = [ptr(l) if len(l) else None for l in self.lists]
         d.kind, d.precision = self.kind, self.precision
         d.degree_mode, d.degree_min = self.degree_mode, self.degree_min
+        d.work_split = self.work_split
         stream = torch.cuda.current_stream(self.device).cuda_stream
         check(load().btk_plan_create(ctypes.byref(self._plan), ctypes.byref(d), stream))
 

@@ -274,7 +274,7 @@ typedef struct {
   const btk_tree_info* tree_source; /* NULL: same tree */
   const void* panels_target;        /* btk_panel_2d[] or btk_panel_3d[] */
   const void* panels_source;        /* NULL: same tree */
-  const int* panel_points_inside_target;
+  const int* panel_points_inside_target; /* NULL (one tree only): leaf order from point_leaf_panel_source */
   const int* panel_points_inside_source; /* NULL: same tree */
   const int* point_leaf_panel_source;
   const btk_interact_pair* pp_list;
@@ -290,6 +290,9 @@ typedef struct {
    * cfg.interp_degree (exact anterpolation/promotion between degrees). */
   int degree_mode;
   int degree_min;
+  /* Work items per persistent-grid slot the interaction scheduler aims at
+   * (source lists of costlier items are cut into pieces); 0 = 8. */
+  int work_split;
 } btk_plan_desc;
 
 enum { BTK_DEGREE_FIXED = 0, BTK_DEGREE_PER_PAIR = 1 };
@@ -415,6 +418,82 @@ btk_status btk_mlp_adam(float* master, void* w_bf16, const float* grad, float* m
  * probe kernel with independent FMA chains on every SM. The roofline
  * denominator for the pairwise interaction kernels. */
 btk_status btk_measure_pipe_peak(int which, double* tflops, btk_stream_t stream);
+
+/* ---- 5. Batches of independent problems ---------------------------------
+ *
+ * No counterpart in the reference (which solves one problem per call). Many
+ * independent problems (targets = sources each) are solved as ONE plan over a
+ * forest: each problem's tree and interaction lists come from the host tree
+ * functions above (bit-identical to the reference's, with that problem's own
+ * leaf size), and the trees are renumbered level by level into one panel
+ * array (all level-0 roots, then all level-1 panels, ...), so the upward
+ * pass, one persistent interaction launch and the downward pass cover every
+ * problem at once. Interaction lists never cross problems. */
+
+typedef struct {
+  int dim, degree;
+  double theta, eps;
+  int n_problems;
+  const int* point_offset; /* n_problems + 1: problem b owns points [off[b], off[b+1]) */
+  const int* cluster_size; /* n_problems: leaf size of each problem's tree */
+} btk_forest_desc;
+
+/* A forest in the reference's layouts. Arrays are allocated by the library
+ * (btk_forest_free). Point indices are global (concatenated order). */
+typedef struct {
+  btk_run_config cfg;        /* dim, degree, theta, eps, thresh = max leaf size, the four list counts */
+  btk_tree_info info;        /* panel_count, levels, level_start[levels + 1] */
+  void* panels;              /* btk_panel_2d / btk_panel_3d [panel_count]; id, parent and children renumbered */
+  int* point_leaf_panel;     /* [total points] forest leaf of each point */
+  int* panel_problem;        /* [panel_count] problem of each panel */
+  int* panel_local;          /* [panel_count] index of the panel in its problem's own tree */
+  btk_interact_pair* pp_list; /* per class: every problem's pairs, problem by problem, renumbered */
+  btk_interact_pair* pc_list;
+  btk_interact_pair* cp_list;
+  btk_interact_pair* cc_list;
+} btk_forest;
+
+/* Builds every problem's tree and lists (host threads in parallel) and the
+ * forest. x, y (, z) are HOST arrays of all points, concatenated. */
+btk_status btk_forest_build(const btk_forest_desc* desc, const double* x, const double* y, const double* z,
+                            btk_forest* forest);
+void btk_forest_free(btk_forest* forest);
+
+typedef struct btk_batch btk_batch;
+
+typedef struct {
+  btk_forest_desc forest;
+  int kind;       /* btk_kind */
+  int precision;  /* btk_precision */
+  int work_split; /* work items per persistent-grid slot (0 = 8) */
+} btk_batch_desc;
+
+/* Builds the forest and its plan and uploads the coordinates (HOST arrays,
+ * concatenated). The geometry is fixed for the batch's life. */
+btk_status btk_batch_create(btk_batch** batch, const btk_batch_desc* desc, const double* x, const double* y,
+                            const double* z, btk_stream_t stream);
+btk_status btk_batch_destroy(btk_batch* batch);
+
+/* One solve of every problem. charges: DEVICE [total points]; out: DEVICE
+ * [ncomp][total points] (OVERWRITTEN), both in the concatenated order. The
+ * whole solve (gathers, upward pass, the persistent interaction launch,
+ * downward pass) is one CUDA graph, captured on the first call (on a stream of
+ * the batch's own) and replayed on `stream` after that; the charges are copied
+ * into the batch's buffer and the result out of it inside the same stream
+ * order. Asynchronous. */
+btk_status btk_batch_execute(btk_batch* batch, const double* charges, double* out, btk_stream_t stream);
+
+typedef struct {
+  int n_problems;
+  int64_t total_points;
+  int panel_count, levels;
+  int64_t evals_pp, evals_pc, evals_cp, evals_cc;
+  int64_t work_items;
+  int graph_kernel_nodes; /* kernels in the captured solve graph (0 before the first execute) */
+  int graph_nodes;        /* all nodes of that graph */
+  float last_ms;          /* device time of the last btk_batch_execute (graph launch only) */
+} btk_batch_stats;
+btk_status btk_batch_stats_get(btk_batch* batch, btk_batch_stats* stats);
 
 #ifdef __cplusplus
 }
