@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
 // FP64 precision; the constant factor is applied in FP64 at the end.
 // ---------------------------------------------------------------------------
 constexpr int kPairs = kChunk / 2;   // source pairs per chunk
-constexpr int kFoldPairs = 64;       // fold FP32 partials into FP64 every 128 sources
+constexpr int kFoldPairs = kPairs;   // fold FP32 partials into FP64 once per chunk (256 sources)
 static_assert(kPairs == kInteractThreads, "one thread converts one source pair per chunk");
 // Padding source for an odd chunk: zero weight, placed 3e18 away (negated
 // relative coordinate), so r^2 stays finite in FP32 and the term is exactly 0.

@@ -71,6 +71,7 @@ struct Side {
   std::vector<int> clusters;      // non-leaf panels, panel order (proxy slots)
   std::vector<int> cluster_slot;  // per panel (-1 for leaves)
   std::vector<std::vector<int>> nonleaf_by_level, panels_by_level;
+  std::vector<int> h_perm;  // leaf-order position -> original index (when built on the host)
   // device
   DevPanel* d_panels = nullptr;
   int *d_leaf_begin = nullptr, *d_point_count = nullptr, *d_leaves = nullptr, *d_clusters = nullptr;
@@ -184,7 +185,8 @@ btk_status side_upload(Side& S, Arena& A, const int* host_inside, const int* dev
   // Leaf order permutation.
   BTK_TRY(A.alloc(&S.d_perm, (size_t)std::max(S.n_points, 1)));
   if (host_inside) {
-    std::vector<int> perm(S.n_points);
+    std::vector<int>& perm = S.h_perm;
+    perm.assign(S.n_points, 0);
     for (int L : S.leaves)
       for (int j = 0; j < h.point_count[L]; ++j) {
         int v = host_inside[(size_t)L * thresh + j];
@@ -203,7 +205,8 @@ btk_status side_upload(Side& S, Arena& A, const int* host_inside, const int* dev
 // ascending original index inside each leaf, the order of panel_points_inside).
 btk_status side_perm_from_leaf_of(Side& S, Arena& A, const std::vector<int>& leaf_of) {
   std::vector<int> cursor(S.leaf_begin);
-  std::vector<int> perm(S.n_points);
+  std::vector<int>& perm = S.h_perm;
+  perm.assign(S.n_points, 0);
   for (int i = 0; i < S.n_points; ++i) {
     int L = leaf_of[i];
     BTK_CHECK(L >= 0 && L < S.h.panel_count && S.h.is_leaf[L], BTK_ERR_INVALID_ARGUMENT,
@@ -576,8 +579,14 @@ void recount_far_evals(btk_plan* P) {
   for (int i = P->n_cp; i < P->n_far; ++i) P->evals[3] += sz(P->h_deg_far[i]) * sz(P->h_deg_far[i]);
 }
 
-void audit_layout(int nt, int ns, int* na, int* tiles, int* pieces);
-btk_status setup_audit(btk_plan* P, Arena& A, int item_base, int entry_base, cudaStream_t st);
+// The audit's targets and work items (built on the host; see build_audit_work).
+struct AuditWork {
+  std::vector<int> orig;  // audited targets (original indices), tile order
+  std::vector<WorkItem> items;
+  std::vector<Entry> entries;
+};
+void build_audit_work(const btk_plan* P, int entry_base, AuditWork& W);
+btk_status setup_audit(btk_plan* P, Arena& A, const AuditWork& W, int item_base, int entry_base, cudaStream_t st);
 
 btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists[4], const int counts[4], int slots,
                                cudaStream_t st) {
@@ -705,13 +714,14 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   BTK_TRY(A.upload(&P->d_far_src, far_src));
   BTK_TRY(A.upload(&P->d_tgt_centre, centre));
   const size_t n_items = (size_t)P->n_static_items + (size_t)P->n_far * P->tiles_max;
-  int a_na, a_tiles, a_pieces;
-  audit_layout(T.n_points, S.n_points, &a_na, &a_tiles, &a_pieces);
-  const size_t n_audit_items = (size_t)a_tiles * a_pieces;
+  AuditWork audit;
+  build_audit_work(P, P->n_static_entries + P->n_far, audit);
+  const size_t n_audit_items = audit.items.size(), n_audit_entries = audit.entries.size();
   BTK_CHECK(n_items + n_audit_items < (1u << 31), BTK_ERR_UNSUPPORTED, "too many work items");
   // items: [static PP/PC | far CP/CC tiles | audit]; entries: [static | far | audit]
   BTK_TRY(A.alloc(&P->ictx.d_items, std::max<size_t>(n_items + n_audit_items, 1)));
-  BTK_TRY(A.alloc(&P->ictx.d_entries, std::max<size_t>((size_t)P->n_static_entries + P->n_far + a_pieces, 1)));
+  BTK_TRY(A.alloc(&P->ictx.d_entries,
+                  std::max<size_t>((size_t)P->n_static_entries + P->n_far + n_audit_entries, 1)));
   if (!W.items.empty())
     BTK_CUDA(cudaMemcpyAsync(P->ictx.d_items, W.items.data(), sizeof(WorkItem) * W.items.size(),
                              cudaMemcpyHostToDevice, st));
@@ -768,7 +778,8 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     }
     P->root_radius = std::max(0.5 * std::sqrt(r2), 1e-300);
   }
-  BTK_TRY(setup_audit(P, A, P->n_items_main, P->n_static_entries + P->n_far, st));
+  BTK_TRY(setup_audit(P, A, audit, P->n_items_main, P->n_static_entries + P->n_far, st));
+  BTK_CUDA(cudaStreamSynchronize(st));  // the copies read the audit's host vectors
   // Work arrays.
   BTK_TRY(A.alloc(&P->d_S4, (size_t)S.n_points + P->total_src_slots + 1));
   BTK_TRY(A.alloc(&P->d_T4, (size_t)T.n_points + P->total_tgt_slots + 1));
@@ -1001,26 +1012,23 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
 
 namespace {
 
-// A fixed, seeded 1% sample of the targets (at least one), and work items for
-// the direct sum over every source: tiles of kTile audited targets times
-// pieces of the sorted source points, all sources on the hi/lo path.
-// Audit layout: na targets (one per 100, at least one when there are
-// targets), kTile targets per tile, the sources cut into pieces of
-// kAuditPiece so the items are small tail-fillers of the solve's launch.
+// The audit: a fixed, seeded 1% sample of the targets (at least one when
+// there are targets) and work items for the FP64-accurate direct sum over every
+// source, built on the host at plan creation. The sampled targets are sorted
+// along the leaf order (a space-filling order of the tree) and cut into tiles
+// of kTile, so a tile covers a compact region; each tile lists the source
+// leaves near its box first (hi/lo coordinate path, as touching PP sources)
+// and the rest after (plain FP32 path, separation at least half the box's
+// side), relative to the box centre, in pieces of about kAuditPiece sources so
+// the items are small tail-fillers of the solve's launch.
 constexpr int kAuditPiece = 4096;
-void audit_layout(int nt, int ns, int* na, int* tiles, int* pieces) {
-  *na = nt > 0 ? std::max(1, nt / 100) : 0;
-  *tiles = (*na + kTile - 1) / kTile;
-  *pieces = ns > 0 ? (ns + kAuditPiece - 1) / kAuditPiece : 0;
-}
 
-// Builds the audit sample and its work items into ictx's arrays at
-// item_base / entry_base (capacity reserved by the caller).
-btk_status setup_audit(btk_plan* P, Arena& A, int item_base, int entry_base, cudaStream_t st) {
-  const int nt = P->tgt.n_points, ns = P->src->n_points;
-  int na, tiles, pieces;
-  audit_layout(nt, ns, &na, &tiles, &pieces);
-  std::vector<int> orig(std::max(na, 1), 0);
+void build_audit_work(const btk_plan* P, int entry_base, AuditWork& W) {
+  const Side& T = P->tgt;
+  const Side& S = *P->src;
+  const int nt = T.n_points;
+  const int na = nt > 0 ? std::max(1, nt / 100) : 0;
+  W.orig.assign(na, 0);
   // Evenly spread, seeded offsets (SplitMix64-style hash) over the index range.
   for (int k = 0; k < na; ++k) {
     uint64_t z = 0x9E3779B97F4A7C15ULL * (uint64_t)(k + 1);
@@ -1028,43 +1036,100 @@ btk_status setup_audit(btk_plan* P, Arena& A, int item_base, int entry_base, cud
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
     z ^= z >> 31;
     const int64_t lo = (int64_t)k * nt / na, hi = (int64_t)(k + 1) * nt / na;
-    orig[k] = (int)(lo + (int64_t)(z % (uint64_t)std::max<int64_t>(1, hi - lo)));
+    W.orig[k] = (int)(lo + (int64_t)(z % (uint64_t)std::max<int64_t>(1, hi - lo)));
   }
-  BTK_TRY(A.upload(&P->d_audit_orig, orig));
+  // Leaf-order position and leaf of every target (when the host knows the order).
+  std::vector<int> pos_of, leaf_at;
+  const bool spatial = (int)T.h_perm.size() == nt && nt > 0;
+  if (spatial) {
+    pos_of.assign(nt, 0);
+    for (int p = 0; p < nt; ++p) pos_of[T.h_perm[p]] = p;
+    leaf_at.assign(nt, -1);
+    for (int L : T.leaves)
+      for (int j = 0; j < T.h.point_count[L]; ++j) leaf_at[T.leaf_begin[L] + j] = L;
+    std::sort(W.orig.begin(), W.orig.end(), [&](int a, int b) { return pos_of[a] < pos_of[b]; });
+  }
+  const int dim = T.h.dim;
+  for (int t0 = 0; t0 < na; t0 += kTile) {
+    const int tc = std::min(kTile, na - t0);
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    if (spatial) {
+      for (int d = 0; d < dim; ++d) {
+        lo[d] = 1e300;
+        hi[d] = -1e300;
+      }
+      for (int k = t0; k < t0 + tc; ++k) {
+        const PanelGeom& g = T.h.geom[leaf_at[pos_of[W.orig[k]]]];
+        for (int d = 0; d < dim; ++d) {
+          lo[d] = std::min(lo[d], g.lo[d]);
+          hi[d] = std::max(hi[d], g.hi[d]);
+        }
+      }
+    } else {
+      for (int d = 0; d < dim; ++d) {
+        lo[d] = S.h.geom[0].lo[d];
+        hi[d] = S.h.geom[0].hi[d];
+      }
+    }
+    double c[3] = {0, 0, 0}, side = 0;
+    for (int d = 0; d < dim; ++d) {
+      c[d] = 0.5 * (lo[d] + hi[d]);
+      side = std::max(side, hi[d] - lo[d]);
+    }
+    // Source leaves: near the tile's box first, then the rest.
+    std::vector<Entry> near, far;
+    for (int L : S.leaves) {
+      const PanelGeom& g = S.h.geom[L];
+      double gap = 0;
+      for (int d = 0; d < dim; ++d) gap = std::max(gap, std::max(g.lo[d] - hi[d], lo[d] - g.hi[d]));
+      (spatial && gap > 0.5 * side ? far : near).push_back(Entry{S.leaf_begin[L], S.h.point_count[L]});
+    }
+    int n_near = 0;
+    for (const Entry& e : near) n_near += e.s_count;
+    const int e_first = (int)W.entries.size();
+    W.entries.insert(W.entries.end(), near.begin(), near.end());
+    W.entries.insert(W.entries.end(), far.begin(), far.end());
+    const int e_last = (int)W.entries.size();
+    int k = e_first, before = 0;  // sources of this tile's list ahead of entry k
+    while (k < e_last) {
+      const int kb = k;
+      int st = 0;
+      while (k < e_last && (st == 0 || st + W.entries[k].s_count <= kAuditPiece)) st += W.entries[k++].s_count;
+      WorkItem w{};
+      w.t_begin = t0;
+      w.t_count = tc;
+      w.e_begin = entry_base + kb;
+      w.e_end = entry_base + k;
+      w.s_total = st;
+      w.flags = kItemAtomic | kItemAudit;
+      w.near_total = std::max(0, std::min(st, n_near - before));
+      w.cx = c[0];
+      w.cy = c[1];
+      w.cz = c[2];
+      W.items.push_back(w);
+      before += st;
+    }
+  }
+}
+
+// Uploads the audit sample and its work items into ictx's arrays at
+// item_base / entry_base (capacity reserved by the caller). The caller
+// synchronises the stream before W goes out of scope.
+btk_status setup_audit(btk_plan* P, Arena& A, const AuditWork& W, int item_base, int entry_base, cudaStream_t st) {
+  const int na = (int)W.orig.size();
+  BTK_TRY(A.upload(&P->d_audit_orig, W.orig.empty() ? std::vector<int>{0} : W.orig));
   BTK_TRY(A.alloc(&P->d_audit_T4, (size_t)std::max(na, 1)));
   BTK_TRY(A.alloc(&P->d_audit_out, (size_t)P->ncomp * std::max(na, 1)));
   BTK_TRY(A.alloc(&P->d_audit_sums, 2));
   BTK_TRY(A.alloc(&P->d_report, kMaxNodes));
-  std::vector<Entry> entries;
-  std::vector<WorkItem> items;
-  for (int p = 0; p < pieces; ++p) {
-    const int b = p * kAuditPiece, e = std::min(ns, b + kAuditPiece);
-    entries.push_back(Entry{b, e - b});
-  }
-  for (int t = 0; t < tiles; ++t)
-    for (int p = 0; p < pieces; ++p) {
-      WorkItem w{};
-      w.t_begin = t * kTile;
-      w.t_count = std::min(kTile, na - t * kTile);
-      w.e_begin = entry_base + p;
-      w.e_end = entry_base + p + 1;
-      w.s_total = entries[p].s_count;
-      w.flags = kItemAtomic | kItemAudit;
-      w.near_total = w.s_total;  // every source takes the hi/lo path
-      w.cx = P->root_centre[0];
-      w.cy = P->root_centre[1];
-      w.cz = P->root_centre[2];
-      items.push_back(w);
-    }
-  if (!items.empty()) {
-    BTK_CUDA(cudaMemcpyAsync(P->ictx.d_items + item_base, items.data(), sizeof(WorkItem) * items.size(),
+  if (!W.items.empty()) {
+    BTK_CUDA(cudaMemcpyAsync(P->ictx.d_items + item_base, W.items.data(), sizeof(WorkItem) * W.items.size(),
                              cudaMemcpyHostToDevice, st));
-    BTK_CUDA(cudaMemcpyAsync(P->ictx.d_entries + entry_base, entries.data(), sizeof(Entry) * entries.size(),
+    BTK_CUDA(cudaMemcpyAsync(P->ictx.d_entries + entry_base, W.entries.data(), sizeof(Entry) * W.entries.size(),
                              cudaMemcpyHostToDevice, st));
-    BTK_CUDA(cudaStreamSynchronize(st));  // the host vectors go out of scope
   }
   P->n_audit = na;
-  P->n_audit_items = (int)items.size();
+  P->n_audit_items = (int)W.items.size();
   return BTK_OK;
 }
 

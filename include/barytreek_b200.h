@@ -414,9 +414,11 @@ btk_status btk_mlp_adam(float* master, void* w_bf16, const float* grad, float* m
                         btk_stream_t stream);
 
 /* Sustained fused-multiply-add rate of this GPU's FP64 (which = 0) or FP32
- * (which = 1) CUDA-core pipe, in TFLOP/s (2 flops per FMA), measured by a
- * probe kernel with independent FMA chains on every SM. The roofline
- * denominator for the pairwise interaction kernels. */
+ * (which = 1: scalar FFMA; which = 2: packed f32x2 FFMA2) CUDA-core pipe, in
+ * TFLOP/s (2 flops per FMA), measured by a probe kernel with independent FMA
+ * chains on every SM; which = 3 gives the MUFU reciprocal-square-root rate in
+ * T results/s. The roofline denominators for the pairwise interaction
+ * kernels. */
 btk_status btk_measure_pipe_peak(int which, double* tflops, btk_stream_t stream);
 
 /* ---- 5. Batches of independent problems ---------------------------------
