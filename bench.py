@@ -402,6 +402,14 @@ def run_native(args, world, rank, local):
         r = forms["learned"].report
         line["learned"] = {k: r[k] for k in ("audit_rel_l2", "audit_targets", "fell_back", "evals_near", "evals_far",
                                              "ms_select", "ms_solve", "ms_kernel", "degree_hist")}
+        # the audit's direct sum runs as items of the same launch
+        audit_evals = r["audit_targets"] * N_POINTS
+        line["learned"]["evals_audit"] = audit_evals
+        flops = FLOPS_PER_EVAL[kind] * (H["evals"] + audit_evals)
+        achieved = flops / (kernel_ms * 1e-3) / 1e12
+        line["roofline"].update({"achieved": achieved, "frac": achieved / peak.value, "flops_per_launch": flops})
+    if not args.no_batch and world == 1:
+        line["batch"] = run_batch(args, flush)
     if world == 1 and not args.no_cpu_baseline:
         from oracle import RefLib
         if RefLib.available():
@@ -420,6 +428,70 @@ def run_native(args, world, rank, local):
     return line
 
 
+def run_batch(args, flush):
+    """The batched workload: 256 independent 3-D Coulomb potential problems,
+    N log-uniform in [4096, 262144], Gaussian-mixture sources, N(0,1) charges,
+    n = 6, theta = 0.6, mixed precision, leaf size and work split per size
+    bucket from the autotuner's table; every solve is one captured graph."""
+    import torch
+    from barytreek_b200 import _lib, batch
+    L = _lib.load()
+    probs = batch.cfg3_problems(SEED)
+    coords = [p[0] for p in probs]
+    q = np.ascontiguousarray(np.concatenate([p[1] for p in probs]))
+    table = batch.Autotuner.load()
+    t0 = time.time()
+    b = batch.Batch(coords, degree=6, theta=0.6, eps=EPS, kind=0, table=table)
+    setup = time.time() - t0
+    qd = torch.from_numpy(q).cuda()
+    out = torch.empty((1, b.n), dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        b.solve(qd, out)
+    torch.cuda.synchronize()
+    launches0 = L.btk_launch_count()
+    ms = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            b.solve(qd, out)
+            ms.append(b.stats()["last_ms"])
+    launches = (L.btk_launch_count() - launches0) / args.steps
+    st = b.stats()
+    evals = b.evals()
+    # accuracy: 64 targets of every 16th problem against the FP64 direct sum over its own sources
+    res = out.cpu().numpy()[0]
+    err2 = ref2 = 0.0
+    for i in range(0, len(probs), 16):
+        pts, qi = probs[i]
+        idx = np.linspace(0, len(qi) - 1, 64).astype(np.int64)
+        t = [torch.from_numpy(np.ascontiguousarray(c[idx])).cuda() for c in pts]
+        s_ = [torch.from_numpy(np.ascontiguousarray(c)).cuda() for c in pts]
+        o = torch.empty((1, len(idx)), dtype=torch.float64, device="cuda")
+        _lib.check(L.btk_direct_sum(3, 0, EPS, len(idx), _lib.ptr(t[0]), _lib.ptr(t[1]), _lib.ptr(t[2]), len(qi),
+                                    _lib.ptr(s_[0]), _lib.ptr(s_[1]), _lib.ptr(s_[2]),
+                                    _lib.ptr(torch.from_numpy(qi).cuda()), _lib.ptr(o), None))
+        d = o.cpu().numpy()[0]
+        err2 += float(np.sum((res[b.offsets[i] + idx] - d) ** 2))
+        ref2 += float(np.sum(d ** 2))
+    m = statistics.median(ms)
+    out_line = {
+        "workload": "256 independent 3-D Coulomb potential problems, N log-uniform in [4096, 262144], "
+                    "Gaussian mixtures of 1-8 components (sigma 0.02-0.2) in the unit cube, N(0,1) charges, "
+                    "n=6, theta=0.6, mixed FP32/FP64",
+        "problems": st["n_problems"], "points": st["total_points"], "ms_per_step": m,
+        "value": evals / (m * 1e-3), "unit": "interactions/s", "evaluations": evals,
+        "graph_kernel_nodes": st["graph_kernel_nodes"], "graph_nodes": st["graph_nodes"],
+        "graph_launches_per_step": 1, "kernel_launches_per_step": launches, "work_items": st["work_items"],
+        "levels": st["levels"], "panels": st["panel_count"], "setup_s": setup,
+        "leaf_size_by_bucket": {f"2^{k}": v[0] for k, v in sorted(table.table.items())},
+        "work_split": b.work_split, "rel_l2_vs_direct_sampled": (err2 / ref2) ** 0.5 if ref2 > 0 else None,
+        "clocks": clk.summary(),
+    }
+    b.close()
+    return out_line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -430,6 +502,7 @@ def main():
     ap.add_argument("--form", default="learned", choices=["plain", "mixed", "learned"],
                     help="the form reported as the headline (all cheaper forms are timed beside it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-problems measurement")
     ap.add_argument("--points", type=int, default=N_POINTS, help="point count (profiling captures only)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
