@@ -160,7 +160,7 @@ class LearnedReport(ctypes.Structure):
     _fields_ = [("audit_rel_l2", ctypes.c_double), ("audit_targets", ctypes.c_int), ("fell_back", ctypes.c_int),
                 ("evals_near", ctypes.c_int64), ("evals_far", ctypes.c_int64), ("ms_select", ctypes.c_float),
                 ("ms_solve", ctypes.c_float), ("ms_total", ctypes.c_float), ("degree_hist", ctypes.c_int * 13),
-                ("ms_kernel", ctypes.c_float)]
+                ("ms_kernel", ctypes.c_float), ("pair_tol", ctypes.c_double)]
 
 _lib = None
 

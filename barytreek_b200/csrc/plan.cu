@@ -532,12 +532,16 @@ struct btk_plan {
   // work items follow the solve's in ictx.d_items, [n_items_main, + n_audit_items)
   int n_audit = 0, n_items_main = 0, n_audit_items = 0;
   int work_split = 8;  // work items per persistent-grid slot
+  double adaptive_pair_tol = 0;  // learned solves with pair_tol <= 0 (0: not yet set)
   int* d_audit_orig = nullptr;
   double4* d_audit_T4 = nullptr;
   double *d_audit_out = nullptr, *d_audit_sums = nullptr;
   int* d_report = nullptr;  // degree histogram (kMaxNodes ints), copied with the audit sums
   int *d_cluster_slot_s = nullptr, *d_cluster_slot_t = nullptr;  // panel -> cluster index (or -1)
 };
+
+// Adaptive learned solves start at this fraction of the tolerance per pair.
+constexpr double kAdaptiveStart = 0.05;
 
 struct btk_selector {
   void* d_w = nullptr;  // BF16 parameters
@@ -1202,7 +1206,9 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   BTK_CHECK(P && sel && xt && yt && xs && ys && charges && out && (P->dim == 2 || (zt && zs)),
             BTK_ERR_INVALID_ARGUMENT, "btk_plan_execute_learned: null argument");
   BTK_CHECK(P->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT, "plan is not BTK_DEGREE_PER_PAIR");
-  BTK_CHECK(tol > 0 && pair_tol > 0, BTK_ERR_INVALID_ARGUMENT, "tolerances must be positive");
+  BTK_CHECK(tol > 0, BTK_ERR_INVALID_ARGUMENT, "tol must be positive");
+  const bool adaptive = !(pair_tol > 0);
+  if (adaptive) pair_tol = P->adaptive_pair_tol > 0 ? P->adaptive_pair_tol : kAdaptiveStart * tol;
   cudaStream_t st = (cudaStream_t)stream;
   Side& T = P->tgt;
   Side& S = *P->src;
@@ -1275,6 +1281,12 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   BTK_CUDA(cudaMemcpyAsync(hist, P->d_report, sizeof(hist), cudaMemcpyDeviceToHost, st));
   BTK_CUDA(cudaStreamSynchronize(st));
   const double rel = std::sqrt(sums[0] / std::max(sums[1], 1e-300));
+  if (adaptive) {
+    // Close the loop on the audit: the global error grows about like
+    // pair_tol^0.7, so this settles near an audit of tol / 2 without overshoot.
+    const double r = rel > 0 ? 0.5 * tol / rel : 2.0;
+    P->adaptive_pair_tol = std::min(tol, std::max(1e-4 * tol, pair_tol * std::min(2.0, std::max(0.5, r))));
+  }
   int fell_back = 0;
   if (!(rel <= tol)) {
     // Fallback: the fixed-degree plain method (degree n everywhere, FP64).
@@ -1298,6 +1310,7 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     cudaEventElapsedTime(&report->ms_total, e[0], e[3]);
     std::memcpy(report->degree_hist, hist, sizeof(hist));
     cudaEventElapsedTime(&report->ms_kernel, ek[0], ek[1]);
+    report->pair_tol = pair_tol;
   }
   for (auto& x : e) cudaEventDestroy(x);
   for (auto& x : ek) cudaEventDestroy(x);

@@ -25,6 +25,14 @@ from ._lib import check, load, ptr
 N_FEATURES, N_HIDDEN, N_OUT, DEG_LO = 16, 64, 9, 4
 WEIGHTS_VERSION = 1
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "selector_weights.npz")
+# The reference's 3-D "velocity" kernel q (t-s)/(r^2+eps^2) has its own far-field
+# error behaviour; its network is trained on its own samples.
+VEL_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "selector_weights_vel.npz")
+
+
+def weights_for(kind: int) -> str:
+    """The weight file for a kernel kind (VEL has its own; POT and FIELD share one)."""
+    return VEL_WEIGHTS if kind == _lib.KIND_VEL else DEFAULT_WEIGHTS
 
 
 def param_count() -> int:
@@ -52,7 +60,9 @@ class Selector:
         self._h = ctypes.c_void_p()
 
     @classmethod
-    def load(cls, path: str = DEFAULT_WEIGHTS) -> "Selector":
+    def load(cls, path: str | None = None, kind: int = _lib.KIND_FIELD) -> "Selector":
+        """Loads a weight file (default: the one for ``kind``)."""
+        path = path or weights_for(kind)
         z = np.load(path, allow_pickle=False)
         if int(z["version"]) != WEIGHTS_VERSION:
             raise ValueError(f"{path}: weight file version {int(z['version'])}, expected {WEIGHTS_VERSION}")

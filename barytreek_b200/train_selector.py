@@ -18,7 +18,7 @@ import time
 import numpy as np
 
 from . import datagen, selector
-from .treecode import Treecode, KIND_FIELD
+from .treecode import Treecode, KIND_FIELD, KIND_VEL
 from ._lib import DEGREE_PER_PAIR
 
 # (family, N, leaf, theta, eps); each is drawn with seeds 1000*r + index, r = 0, 1, ...
@@ -37,6 +37,8 @@ BASE = [
     ("sphere", 1 << 18, 1000, 0.7, 1e-4),
     ("mixture", 1 << 19, 1500, 0.6, 1e-4),
     ("mixture", 1 << 18, 600, 0.7, 1e-4),
+    ("plummer", 1 << 21, 2000, 0.7, 1e-4),
+    ("sphere", 1 << 21, 2000, 0.8, 1e-3),
 ]
 
 
@@ -50,7 +52,7 @@ def problem(family, n, seed):
     return datagen.gaussian_mixture(seed, n)
 
 
-def collect(n_total, K=16, log=print, max_rounds=12):
+def collect(n_total, K=16, log=print, max_rounds=12, kind=KIND_FIELD):
     # at most this many pairs from one problem, so every family contributes
     per_problem = max(20000, n_total // (2 * len(BASE)))
     Xs, Es, got = [], [], 0
@@ -61,7 +63,7 @@ def collect(n_total, K=16, log=print, max_rounds=12):
             seed = 1000 * r + 10 + i
             t0 = time.time()
             pts, q = problem(fam, n, seed)
-            tc = Treecode(pts, degree=12, cluster_size=leaf, theta=theta, eps=eps, kind=KIND_FIELD,
+            tc = Treecode(pts, degree=12, cluster_size=leaf, theta=theta, eps=eps, kind=kind,
                           degree_mode=DEGREE_PER_PAIR, degree_min=4)
             X, E = selector.generate_samples(tc, q, min(per_problem, n_total - got), K=K, seed=seed)
             tc.close()
@@ -75,24 +77,27 @@ def collect(n_total, K=16, log=print, max_rounds=12):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=selector.DEFAULT_WEIGHTS)
+    ap.add_argument("--kind", type=int, default=KIND_FIELD, choices=[KIND_FIELD, KIND_VEL],
+                    help="kernel kind of the error samples (2 FIELD, also used for POT; 1 VEL)")
+    ap.add_argument("--out", default=None, help="weight file (default: the package's file for --kind)")
     ap.add_argument("--samples", type=int, default=2_000_000)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--cache", default=None, help="sample cache (.npz); reused when present")
     args = ap.parse_args()
+    args.out = args.out or selector.weights_for(args.kind)
     cache = args.cache or os.path.splitext(args.out)[0] + "_samples.npz"
     if os.path.exists(cache):
         z = np.load(cache)
         X, E = z["X"], z["E"]
         print(f"loaded {len(X)} samples from {cache}")
     else:
-        X, E = collect(args.samples)
+        X, E = collect(args.samples, kind=args.kind)
         np.savez(cache, X=X, E=E)
     Y, M = selector.to_targets(E, 4, 12)
     sel = selector.train(X, Y, M, epochs=args.epochs, batch=args.batch, lr=args.lr, log=print)
-    sel.meta.update({"families": ",".join(f"{f}:{n}:{l}:{t}" for f, n, l, t, _ in BASE)})
+    sel.meta.update({"families": ",".join(f"{f}:{n}:{l}:{t}" for f, n, l, t, _ in BASE), "kind": args.kind})
     sel.save(args.out)
     print(f"wrote {args.out}: {sel.meta}")
 

@@ -229,7 +229,7 @@ class Treecode:
         q = q.to(self.device, torch.float64).contiguous()
         if out is None:
             out = torch.empty((self.ncomp, self.nt), dtype=torch.float64, device=self.device)
-        pair_tol = tol * 0.05 if pair_tol is None else pair_tol
+        pair_tol = 0.0 if pair_tol is None else pair_tol  # 0: the plan's adaptive per-pair tolerance
         t, s = self._t, self._s
         stream = torch.cuda.current_stream(self.device).cuda_stream
         z_t = ptr(t[2]) if self.dim == 3 else None

@@ -251,7 +251,7 @@ class Form:
         else:
             self.tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind,
                                    precision=btk.PREC_MIXED, degree_mode=btk._lib.DEGREE_PER_PAIR, degree_min=4)
-            self.sel = selector.Selector.load()
+            self.sel = selector.Selector.load(kind=kind)
         self.report = None
 
     def step(self, qd, out=None, coords=None):
@@ -263,13 +263,13 @@ class Form:
             out = tc.solve(qd, out)
             t = tc.last_timing()
             return out, t["total"], t["interaction_kernel"], tc.evals(), t
-        out, rep = tc.solve_learned(qd, self.sel, tol=TOL, pair_tol=TOL * PAIR_TOL_FACTOR, degree_lo=4, out=out)
+        # pair_tol=None: the plan's adaptive per-pair tolerance, steered by each solve's audit
+        out, rep = tc.solve_learned(qd, self.sel, tol=TOL, pair_tol=None, degree_lo=4, out=out)
         self.report = rep
         return out, rep["ms_total"], rep["ms_kernel"], rep["evals_near"] + rep["evals_far"], rep
 
 
 TOL = 1e-6
-PAIR_TOL_FACTOR = 0.1
 
 
 def time_form(form, qd, flush, args, world, local):
@@ -376,7 +376,8 @@ def run_native(args, world, rank, local):
         "vs_baseline": None, "dtype": "f64" if headline == "plain" else "f32+f64",
         "data": "synthetic: seeded SplitMix64, uniform unit cube, charges U[-1,1]",
         "config": {"workload": workload_name(kind, 0 if headline == "plain" else 1) +
-                   (", learned per-pair degrees 4..8 with 1% direct-sum audit" if headline == "learned" else ""),
+                   (", learned per-pair degrees 4..8 (adaptive pair tolerance) with 1% direct-sum audit"
+                    if headline == "learned" else ""),
                    "form": headline, "tolerance_rel_l2": TOL,
                    "value_definition": "interactions of the plain fixed-degree solve of this workload "
                                        "(pairwise evaluations at n=8) divided by the solve time of the reported form",
@@ -401,7 +402,7 @@ def run_native(args, world, rank, local):
     if headline == "learned":
         r = forms["learned"].report
         line["learned"] = {k: r[k] for k in ("audit_rel_l2", "audit_targets", "fell_back", "evals_near", "evals_far",
-                                             "ms_select", "ms_solve", "ms_kernel", "degree_hist")}
+                                             "ms_select", "ms_solve", "ms_kernel", "degree_hist", "pair_tol")}
         # the audit's direct sum runs as items of the same launch
         audit_evals = r["audit_targets"] * N_POINTS
         line["learned"]["evals_audit"] = audit_evals

@@ -370,7 +370,8 @@ typedef struct {
   float ms_solve;      /* interactions + promotion + downward at the chosen degrees */
   float ms_total;      /* everything, audit and fallback included */
   int degree_hist[13]; /* far-field pairs per chosen degree */
-  float ms_kernel;     /* the interaction kernel of the learned solve alone */
+  float ms_kernel;     /* the interaction kernel of the learned solve (audit items included) */
+  double pair_tol;     /* the per-pair tolerance this solve used */
 } btk_learned_report;
 
 /* Learned-degree solve: upward pass, features, network, per-pair degree =
@@ -379,7 +380,11 @@ typedef struct {
  * precision), downward pass; then a direct-sum audit of 1% of the targets.
  * When the audit's relative L2 exceeds tol, the fixed-degree FP64 result is
  * computed and returned instead (report->fell_back = 1). Synchronises the
- * stream once (to read the audit). out as btk_plan_execute. */
+ * stream once (to read the audit). out as btk_plan_execute.
+ * pair_tol <= 0 selects the plan's adaptive per-pair tolerance: it starts at
+ * 0.05 tol, and after every such solve it is scaled by (tol/2) / audit
+ * (clamped to [0.5, 2]), so repeated solves on one plan settle where the
+ * audit reads about half the requested tolerance. */
 btk_status btk_plan_execute_learned(btk_plan* plan, const btk_selector* sel, double tol, double pair_tol,
                                     int degree_lo, const double* xt, const double* yt, const double* zt,
                                     const double* xs, const double* ys, const double* zs, const double* charges,

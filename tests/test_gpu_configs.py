@@ -1,0 +1,95 @@
+"""The workload configurations beside the benchmark's, at full size.
+
+* 2-D, N = 65,536 uniform in [-1,1]^2, charges U[-1,1], n = 8, theta = 0.7,
+  leaf 500, potential: the plain FP64 solve against the reference library
+  (relative L2 <= 1e-12) and against the FP64 direct sum.
+* 3-D potential + gradient, N = 4,194,304 Plummer sphere (scale 0.1, truncated
+  at r = 2), charges U[0,1]: the learned-degree mixed solve (adaptive pair
+  tolerance, plan degree 10) against plain FP64 at n = 10.
+* The reference's 3-D vector kernel, eps = 1e-3, N = 2,097,152 on the unit
+  sphere, strengths U[-1,1], theta = 0.8: learned + mixed against plain FP64
+  at n = 10.
+
+For the learned solves, after two settling solves the third must pass its
+audit without falling back, meet 1e-6 relative L2 against the FP64 direct sum
+at 2,000 sampled targets, and run faster than the plain solve.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def _direct(tc, q, kind, eps, m=2000):
+    import torch
+    from barytreek_b200 import _lib
+    L = _lib.load()
+    idx = np.sort(np.random.default_rng(99).choice(tc.nt, m, replace=False))
+    t = [torch.from_numpy(np.ascontiguousarray(c[idx])).cuda() for c in tc.targets]
+    out = torch.empty((tc.ncomp, m), dtype=torch.float64, device="cuda")
+    qd = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    s = tc._t
+    z = lambda a: _lib.ptr(a[2]) if tc.dim == 3 else None
+    _lib.check(L.btk_direct_sum(tc.dim, kind, eps, m, _lib.ptr(t[0]), _lib.ptr(t[1]), z(t), tc.nt, _lib.ptr(s[0]),
+                                _lib.ptr(s[1]), z(s), _lib.ptr(qd), _lib.ptr(out), None))
+    return idx, out.cpu().numpy()
+
+
+def test_2d_65k_matches_reference(reflib):
+    import barytreek_b200 as btk
+    from barytreek_b200 import datagen
+    pts, q = datagen.uniform_box(1, 65536, 2, -1.0, 1.0)
+    tc = btk.Treecode(pts, degree=8, cluster_size=500, theta=0.7, eps=1e-4, kind=btk.KIND_POT)
+    out = tc.solve(q).cpu().numpy()
+    reflib.set_threads(os.cpu_count() or 1)
+    try:
+        rt = reflib.create(2, pts, degree=8, cluster_size=500, theta=0.7, eps=1e-4)
+        ref = rt.solve(0, q, fixed=True)["out"]
+    finally:
+        reflib.set_threads(1)
+    assert rel(out[0], ref[0]) <= 1e-12
+    idx, ds = _direct(tc, q, 0, 1e-4)
+    assert rel(out[:, idx], ds) <= 1e-6
+
+
+def _learned_vs_plain(pts, q, kind, eps, theta, kind_name):
+    import torch
+
+    import barytreek_b200 as btk
+    from barytreek_b200 import selector
+    qd = torch.from_numpy(q).cuda()
+    plain = btk.Treecode(pts, degree=10, cluster_size=2000, theta=theta, eps=eps, kind=kind)
+    plain.solve(qd)
+    plain.solve(qd)
+    torch.cuda.synchronize()
+    plain_ms = plain.last_timing()["total"]
+    idx, ds = _direct(plain, q, kind, eps)
+    plain.close()
+    lt = btk.Treecode(pts, degree=10, cluster_size=2000, theta=theta, eps=eps, kind=kind, precision=btk.PREC_MIXED,
+                      degree_mode=btk._lib.DEGREE_PER_PAIR, degree_min=4)
+    sel = selector.Selector.load(kind=kind)
+    for _ in range(3):
+        out, rep = lt.solve_learned(qd, sel, tol=1e-6)
+    err = rel(out.cpu().numpy()[:, idx], ds)
+    assert rep["fell_back"] == 0, (kind_name, rep)
+    assert rep["audit_rel_l2"] <= 1e-6
+    assert err <= 1e-6, (kind_name, err)
+    assert rep["ms_total"] < plain_ms, (kind_name, rep["ms_total"], plain_ms)
+
+
+def test_plummer_4m_learned_vs_plain_n10():
+    from barytreek_b200 import datagen
+    pts, q = datagen.plummer(1, 1 << 22)
+    _learned_vs_plain(pts, q, 2, 1e-4, 0.7, "plummer field")
+
+
+def test_sphere_2m_vel_learned_vs_plain_n10():
+    from barytreek_b200 import datagen
+    pts, q = datagen.sphere_surface(1, 1 << 21)
+    _learned_vs_plain(pts, q, 1, 1e-3, 0.8, "sphere vel")
