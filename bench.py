@@ -437,7 +437,7 @@ def run_batch(args, flush):
     import torch
     from barytreek_b200 import _lib, batch
     L = _lib.load()
-    probs = batch.cfg3_problems(SEED)
+    probs = batch.cfg3_problems(SEED, count=args.batch_problems)
     coords = [p[0] for p in probs]
     q = np.ascontiguousarray(np.concatenate([p[1] for p in probs]))
     table = batch.Autotuner.load()
@@ -477,7 +477,7 @@ def run_batch(args, flush):
         ref2 += float(np.sum(d ** 2))
     m = statistics.median(ms)
     out_line = {
-        "workload": "256 independent 3-D Coulomb potential problems, N log-uniform in [4096, 262144], "
+        "workload": f"{len(probs)} independent 3-D Coulomb potential problems, N log-uniform in [4096, 262144], "
                     "Gaussian mixtures of 1-8 components (sigma 0.02-0.2) in the unit cube, N(0,1) charges, "
                     "n=6, theta=0.6, mixed FP32/FP64",
         "problems": st["n_problems"], "points": st["total_points"], "ms_per_step": m,
@@ -504,6 +504,8 @@ def main():
                     help="the form reported as the headline (all cheaper forms are timed beside it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-problems measurement")
+    ap.add_argument("--batch-only", action="store_true", help="only the batched-problems measurement (profiling)")
+    ap.add_argument("--batch-problems", type=int, default=256, help="problems in the batch (profiling captures)")
     ap.add_argument("--points", type=int, default=N_POINTS, help="point count (profiling captures only)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -514,7 +516,11 @@ def main():
         line = run_reference(args, world, rank)
     else:
         world, rank, local = dist_setup(args.gpus)
-        line = run_native(args, world, rank, local)
+        if args.batch_only:
+            import torch
+            line = run_batch(args, torch.empty(32 << 20, dtype=torch.float64, device="cuda")) if rank == 0 else None
+        else:
+            line = run_native(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
