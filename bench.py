@@ -139,13 +139,8 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from barytreek_b200.distributed import reduce_over_ranks
+    return reduce_over_ranks(x, "max") if world > 1 else x
 
 
 # ---------------------------------------------------------------- reference arm
@@ -354,6 +349,8 @@ def run_native(args, world, rank, local):
     ref_out = H["out"].cpu().numpy()
     assert np.linalg.norm(h_out.numpy() - ref_out) <= 1e-6 * np.linalg.norm(ref_out)
 
+    # every rank takes part in the batch measurement (its shard of the problems)
+    batch_line = run_batch(args, flush) if not args.no_batch else None
     if rank != 0:
         return None
     idx, ds = direct_check(f.tc, q, kind)
@@ -409,8 +406,8 @@ def run_native(args, world, rank, local):
         flops = FLOPS_PER_EVAL[kind] * (H["evals"] + audit_evals)
         achieved = flops / (kernel_ms * 1e-3) / 1e12
         line["roofline"].update({"achieved": achieved, "frac": achieved / peak.value, "flops_per_launch": flops})
-    if not args.no_batch and world == 1:
-        line["batch"] = run_batch(args, flush)
+    if batch_line is not None:
+        line["batch"] = batch_line
     if world == 1 and not args.no_cpu_baseline:
         from oracle import RefLib
         if RefLib.available():
@@ -436,8 +433,13 @@ def run_batch(args, flush):
     bucket from the autotuner's table; every solve is one captured graph."""
     import torch
     from barytreek_b200 import _lib, batch
+    from barytreek_b200 import distributed as D
     L = _lib.load()
-    probs = batch.cfg3_problems(SEED, count=args.batch_problems)
+    world, rank = D.world_info()
+    all_probs = batch.cfg3_problems(SEED, count=args.batch_problems)
+    # one batch per rank: its size-balanced share of the problems (strong scaling)
+    mine = D.shard_problems([len(p[1]) for p in all_probs], world)[rank]
+    probs = [all_probs[b] for b in mine]
     coords = [p[0] for p in probs]
     q = np.ascontiguousarray(np.concatenate([p[1] for p in probs]))
     table = batch.Autotuner.load()
@@ -449,17 +451,19 @@ def run_batch(args, flush):
     for _ in range(args.warmup):
         b.solve(qd, out)
     torch.cuda.synchronize()
+    barrier(world)
     launches0 = L.btk_launch_count()
     ms = []
-    with ClockSampler(0) as clk:
+    with ClockSampler(torch.cuda.current_device()) as clk:
         for _ in range(args.steps):
             flush_l2(flush)
             torch.cuda.synchronize()
             b.solve(qd, out)
             ms.append(b.stats()["last_ms"])
+    torch.cuda.synchronize()
     launches = (L.btk_launch_count() - launches0) / args.steps
     st = b.stats()
-    evals = b.evals()
+    evals = D.reduce_over_ranks(b.evals(), "sum")
     # accuracy: 64 targets of every 16th problem against the FP64 direct sum over its own sources
     res = out.cpu().numpy()[0]
     err2 = ref2 = 0.0
@@ -475,12 +479,14 @@ def run_batch(args, flush):
         d = o.cpu().numpy()[0]
         err2 += float(np.sum((res[b.offsets[i] + idx] - d) ** 2))
         ref2 += float(np.sum(d ** 2))
-    m = statistics.median(ms)
+    err2, ref2 = D.reduce_over_ranks(err2, "sum"), D.reduce_over_ranks(ref2, "sum")
+    m = D.reduce_over_ranks(sum(ms), "max") / len(ms)  # device time, max over ranks
     out_line = {
-        "workload": f"{len(probs)} independent 3-D Coulomb potential problems, N log-uniform in [4096, 262144], "
+        "workload": f"{len(all_probs)} independent 3-D Coulomb potential problems, N log-uniform in [4096, 262144], "
                     "Gaussian mixtures of 1-8 components (sigma 0.02-0.2) in the unit cube, N(0,1) charges, "
                     "n=6, theta=0.6, mixed FP32/FP64",
-        "problems": st["n_problems"], "points": st["total_points"], "ms_per_step": m,
+        "problems": len(all_probs), "points": int(sum(len(p[1]) for p in all_probs)), "ms_per_step": m,
+        "scaling": "strong", "sharding": f"problems split over {world} rank(s) by point count",
         "value": evals / (m * 1e-3), "unit": "interactions/s", "evaluations": evals,
         "graph_kernel_nodes": st["graph_kernel_nodes"], "graph_nodes": st["graph_nodes"],
         "graph_launches_per_step": 1, "kernel_launches_per_step": launches, "work_items": st["work_items"],
@@ -518,7 +524,8 @@ def main():
         world, rank, local = dist_setup(args.gpus)
         if args.batch_only:
             import torch
-            line = run_batch(args, torch.empty(32 << 20, dtype=torch.float64, device="cuda")) if rank == 0 else None
+            line = run_batch(args, torch.empty(32 << 20, dtype=torch.float64, device="cuda"))
+            line = line if rank == 0 else None
         else:
             line = run_native(args, world, rank, local)
         if world > 1:
