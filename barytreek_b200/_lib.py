@@ -112,6 +112,8 @@ SIGNATURES = {
     "btk_read_run_config": [ctypes.c_char_p, _PRC],
     "btk_tree_construction_2d": [_PRC, _PTI, _vp, _vp, _ci, _vp, _vp, _vp],
     "btk_tree_construction_3d": [_PRC, _PTI, _vp, _vp, _vp, _ci, _vp, _vp, _vp],
+    "btk_tree_construction_2d_device": [_PRC, _PTI, _vp, _vp, _ci, _vp, _vp, _vp, _vp],
+    "btk_tree_construction_3d_device": [_PRC, _PTI, _vp, _vp, _vp, _ci, _vp, _vp, _vp, _vp],
     "btk_dual_tree_traversal_2d": [_PRC, _vp, _vp, _vp],
     "btk_dual_tree_traversal_3d": [_PRC, _vp, _vp, _vp],
     "btk_split_interactions": [_vp, _ci, _vp, _vp, _vp, _vp],

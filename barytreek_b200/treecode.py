@@ -10,7 +10,6 @@ a resident plan.
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass
 
 import numpy as np
 
@@ -51,14 +50,41 @@ def read_run_config(path: str, dim: int) -> RunConfig:
     return cfg
 
 
-@dataclass
 class HostTree:
-    """Output of tree_construction: reference layouts as numpy arrays."""
-    dim: int
-    panels: np.ndarray          # PANEL2_DTYPE / PANEL3_DTYPE records
-    level_start: np.ndarray     # int32[levels+1]
-    point_leaf_panel: np.ndarray  # int32[n]
-    panel_points_inside: np.ndarray  # int32[panel_count, thresh]
+    """Output of tree_construction: reference layouts as numpy arrays.
+
+    panels (PANEL2_DTYPE / PANEL3_DTYPE records), level_start int32[levels+1],
+    point_leaf_panel int32[n], panel_points_inside int32[panel_count, thresh].
+    A tree built on the device carries its leaf rows as ``leaf_order`` (the
+    rows concatenated) and forms panel_points_inside only when asked.
+    """
+
+    def __init__(self, dim, panels, level_start, point_leaf_panel, panel_points_inside=None, leaf_order=None,
+                 thresh=None):
+        self.dim = dim
+        self.panels = panels
+        self.level_start = level_start
+        self.point_leaf_panel = point_leaf_panel
+        self._inside = panel_points_inside
+        self.leaf_order = leaf_order
+        self.thresh = thresh if thresh is not None else (panel_points_inside.shape[1] if panel_points_inside is not None
+                                                         else 0)
+
+    @property
+    def has_inside(self) -> bool:
+        return self._inside is not None
+
+    @property
+    def panel_points_inside(self) -> np.ndarray:
+        if self._inside is None:
+            inside = np.zeros((len(self.panels), self.thresh), np.int32)
+            off = 0
+            for i in np.flatnonzero(self.panels["is_leaf"] != 0):
+                c = int(self.panels["point_count"][i])
+                inside[i, :c] = self.leaf_order[off:off + c]
+                off += c
+            self._inside = inside
+        return self._inside
 
     @property
     def panel_count(self) -> int:
@@ -81,6 +107,36 @@ def _copy_out(addr: int, dtype, count: int) -> np.ndarray:
     if count:
         ctypes.memmove(out.ctypes.data, addr, out.nbytes)
     return out
+
+
+def tree_construction_device(cfg: RunConfig, coords, stream=None) -> HostTree:
+    """The same tree from CUDA-tensor coordinates (btk_tree_construction_*_device):
+    point work on the GPU; panels and leaf rows returned to the host."""
+    import torch
+    L = load()
+    dim = cfg.dim
+    n = int(coords[0].numel())
+    dev = coords[0].device
+    leaf_of = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    order = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    info = TreeInfo()
+    panels_p = ctypes.c_void_p()
+    st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    if dim == 2:
+        check(L.btk_tree_construction_2d_device(ctypes.byref(cfg), ctypes.byref(info), ptr(coords[0]), ptr(coords[1]),
+                                                n, ctypes.byref(panels_p), ptr(leaf_of), ptr(order), st))
+    else:
+        check(L.btk_tree_construction_3d_device(ctypes.byref(cfg), ctypes.byref(info), ptr(coords[0]), ptr(coords[1]),
+                                                ptr(coords[2]), n, ctypes.byref(panels_p), ptr(leaf_of), ptr(order),
+                                                st))
+    try:
+        panels = _copy_out(panels_p.value, PANEL2_DTYPE if dim == 2 else PANEL3_DTYPE, info.panel_count)
+        ls = _copy_out(ctypes.cast(info.level_start, ctypes.c_void_p).value, np.int32, info.levels + 1)
+    finally:
+        L.btk_free(panels_p)
+        L.btk_free(ctypes.cast(info.level_start, ctypes.c_void_p))
+    return HostTree(dim, panels, ls, leaf_of[:n].cpu().numpy(), leaf_order=order[:n].cpu().numpy(),
+                    thresh=cfg.fmm_cluster_thresh)
 
 
 def tree_construction(cfg: RunConfig, coords) -> HostTree:
@@ -136,14 +192,16 @@ class Treecode:
     """A resident treecode plan: targets = sources unless ``sources`` is given.
 
     ``coords``: tuple of dim float64 arrays (host). Trees and lists are built
-    on the host with the bit-identical host functions, then a device plan holds
-    the leaf ordering, geometry and interaction work lists. :meth:`solve` takes
+    with the bit-identical host functions (``device_tree=True``: the same tree
+    built from the device copies of the points), then a device plan holds the
+    leaf ordering, geometry and interaction work lists. :meth:`solve` takes
     charges (numpy or a CUDA tensor) and returns a CUDA tensor
     ``[ncomp, n_targets]`` in the original point order.
     """
 
     def __init__(self, coords, sources=None, *, degree=8, cluster_size=100, theta=0.7, eps=1e-4, kind=KIND_POT,
-                 precision=PREC_FP64, degree_mode=_lib.DEGREE_FIXED, degree_min=1, work_split=0, device="cuda"):
+                 precision=PREC_FP64, degree_mode=_lib.DEGREE_FIXED, degree_min=1, work_split=0, device_tree=False,
+                 device="cuda"):
         import torch
 
         self.dim = len(coords)
@@ -154,15 +212,17 @@ class Treecode:
         self.cfg = make_run_config(self.dim, degree, cluster_size, theta, eps)
         self.targets = tuple(np.ascontiguousarray(c, np.float64) for c in coords)
         self.sources = tuple(np.ascontiguousarray(c, np.float64) for c in sources) if sources is not None else None
-        self.tree_t = tree_construction(self.cfg, self.targets)
+        self.device = torch.device(device)
+        dev = self.device
+        self._t = [torch.from_numpy(c).to(dev) for c in self.targets]
+        # device_tree: the same tree built from the device copies of the points
+        self.tree_t = (tree_construction_device(self.cfg, self._t) if device_tree
+                       else tree_construction(self.cfg, self.targets))
         self.tree_s = tree_construction(self.cfg, self.sources) if self.sources is not None else None
         self.interactions = dual_tree_traversal(self.cfg, self.tree_t, self.tree_s)
         self.lists = split_interactions(self.cfg, self.interactions)
         self.nt = len(self.targets[0])
         self.ns = len(self.sources[0]) if self.sources is not None else self.nt
-        self.device = torch.device(device)
-        dev = self.device
-        self._t = [torch.from_numpy(c).to(dev) for c in self.targets]
         self._s = [torch.from_numpy(c).to(dev) for c in self.sources] if self.sources is not None else self._t
         self._plan = ctypes.c_void_p()
         self._create_plan()
@@ -176,7 +236,9 @@ class Treecode:
         self._ti_t = self.tree_t.tree_info()
         d.tree_target = ctypes.pointer(self._ti_t)
         d.panels_target = ptr(self.tree_t.panels)
-        d.panel_points_inside_target = ptr(self.tree_t.panel_points_inside)
+        # a device-built tree hands over its leaf order through point_leaf_panel (one tree)
+        d.panel_points_inside_target = (ptr(self.tree_t.panel_points_inside)
+                                        if self.tree_t.has_inside or self.tree_s is not None else None)
         src = self.tree_s or self.tree_t
         if self.tree_s is not None:
             self._ti_s = self.tree_s.tree_info()

@@ -137,6 +137,24 @@ btk_status btk_tree_construction_3d(const btk_run_config* cfg, btk_tree_info* in
                                     const double* ycos, const double* zcos, int point_count, btk_panel_3d** panels,
                                     int* point_leaf_panel, int** panel_points_inside);
 
+/* The same trees as btk_tree_construction_2d/3d (every panel field, the level
+ * starts and point_leaf_panel bit-identical), built from DEVICE coordinates:
+ * the point work (root box reduction, the stable per-level partition of the
+ * points into children) runs on the GPU, the per-panel bookkeeping on the
+ * host. Outputs: *panels and info->level_start host arrays allocated by the
+ * library (btk_free); point_leaf_panel[point_count] DEVICE; leaf_order
+ * (DEVICE, point_count ints, may be NULL): the point indices leaf by leaf in
+ * panel order, each leaf ascending -- the rows of panel_points_inside
+ * concatenated without the padding. Synchronises the stream once per tree
+ * level. No counterpart in the reference (whose construction is host code). */
+btk_status btk_tree_construction_2d_device(const btk_run_config* cfg, btk_tree_info* info, const double* xcos,
+                                           const double* ycos, int point_count, btk_panel_2d** panels,
+                                           int* point_leaf_panel, int* leaf_order, btk_stream_t stream);
+btk_status btk_tree_construction_3d_device(const btk_run_config* cfg, btk_tree_info* info, const double* xcos,
+                                           const double* ycos, const double* zcos, int point_count,
+                                           btk_panel_3d** panels, int* point_leaf_panel, int* leaf_order,
+                                           btk_stream_t stream);
+
 /* src/interaction_list.cpp:5-117 / :119-250. Updates cfg's interaction
  * counts; *interaction_list (cfg->fmm_interaction_count pairs) is allocated
  * by the library (btk_free). */
