@@ -116,6 +116,8 @@ SIGNATURES = {
     "btk_tree_construction_3d_device": [_PRC, _PTI, _vp, _vp, _vp, _ci, _vp, _vp, _vp, _vp],
     "btk_dual_tree_traversal_2d": [_PRC, _vp, _vp, _vp],
     "btk_dual_tree_traversal_3d": [_PRC, _vp, _vp, _vp],
+    "btk_dual_tree_traversal_2d_device": [_PRC, _vp, _ci, _vp, _ci, _vp, _vp],
+    "btk_dual_tree_traversal_3d_device": [_PRC, _vp, _ci, _vp, _ci, _vp, _vp],
     "btk_split_interactions": [_vp, _ci, _vp, _vp, _vp, _vp],
     "btk_upward_pass_2d": [_PRC, _PTI, _vp, _vp, _vp, _vp, _vp, _vp, _ci, _vp],
     "btk_upward_pass_3d": [_PRC, _PTI, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _ci, _vp],

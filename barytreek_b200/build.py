@@ -22,9 +22,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
 # Host tree code must evaluate every expression exactly as written (bit-identical
 # trees and lists): no contraction into fused multiply-adds.
-PER_FILE = {"host_tree.cpp": ["-Xcompiler", "-ffp-contract=off"], "tree_device.cu": ["-Xcompiler", "-ffp-contract=off"]}
+PER_FILE = {"host_tree.cpp": ["-Xcompiler", "-ffp-contract=off"], "tree_device.cu": ["-Xcompiler", "-ffp-contract=off"],
+            "traverse_device.cu": ["-Xcompiler", "-ffp-contract=off"]}
 SOURCES = ["host_tree.cpp", "plan.cu", "kernels_updown.cu", "kernels_interact.cu", "kernels_direct.cu",
-           "kernels_probe.cu", "kernels_degree.cu", "selector.cu", "direct_noalloc.cu", "batch.cpp", "tree_device.cu"]
+           "kernels_probe.cu", "kernels_degree.cu", "selector.cu", "direct_noalloc.cu", "batch.cpp", "tree_device.cu", "traverse_device.cu"]
 HEADERS = ["btk_internal.h", "kernels.cuh", "device_math.cuh"]
 
 

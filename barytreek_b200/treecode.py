@@ -180,6 +180,24 @@ def dual_tree_traversal(cfg: RunConfig, target: HostTree, source: HostTree | Non
         L.btk_free(out)
 
 
+def dual_tree_traversal_device(cfg: RunConfig, target: HostTree, source: HostTree | None = None,
+                               stream=None) -> np.ndarray:
+    """The same list as dual_tree_traversal, computed on the GPU
+    (btk_dual_tree_traversal_*_device); updates cfg's counts."""
+    import torch
+    L = load()
+    source = source or target
+    out = ctypes.c_void_p()
+    fn = L.btk_dual_tree_traversal_2d_device if cfg.dim == 2 else L.btk_dual_tree_traversal_3d_device
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    check(fn(ctypes.byref(cfg), ptr(target.panels), target.panel_count, ptr(source.panels), source.panel_count,
+             ctypes.byref(out), st))
+    try:
+        return _copy_out(out.value, PAIR_DTYPE, cfg.fmm_interaction_count)
+    finally:
+        L.btk_free(out)
+
+
 def split_interactions(cfg: RunConfig, interactions: np.ndarray):
     """split_interactions (src/interaction_list.cpp:252-277) -> (pp, pc, cp, cc)."""
     lists = [np.zeros(c, PAIR_DTYPE) for c in (cfg.fmm_pp_count, cfg.fmm_pc_count, cfg.fmm_cp_count,
@@ -193,7 +211,7 @@ class Treecode:
 
     ``coords``: tuple of dim float64 arrays (host). Trees and lists are built
     with the bit-identical host functions (``device_tree=True``: the same tree
-    built from the device copies of the points), then a device plan holds the
+    and lists built on the GPU from the device copies of the points), then a device plan holds the
     leaf ordering, geometry and interaction work lists. :meth:`solve` takes
     charges (numpy or a CUDA tensor) and returns a CUDA tensor
     ``[ncomp, n_targets]`` in the original point order.
@@ -219,7 +237,8 @@ class Treecode:
         self.tree_t = (tree_construction_device(self.cfg, self._t) if device_tree
                        else tree_construction(self.cfg, self.targets))
         self.tree_s = tree_construction(self.cfg, self.sources) if self.sources is not None else None
-        self.interactions = dual_tree_traversal(self.cfg, self.tree_t, self.tree_s)
+        self.interactions = (dual_tree_traversal_device(self.cfg, self.tree_t, self.tree_s) if device_tree
+                             else dual_tree_traversal(self.cfg, self.tree_t, self.tree_s))
         self.lists = split_interactions(self.cfg, self.interactions)
         self.nt = len(self.targets[0])
         self.ns = len(self.sources[0]) if self.sources is not None else self.nt

@@ -163,6 +163,22 @@ btk_status btk_dual_tree_traversal_2d(btk_run_config* cfg, const btk_panel_2d* p
 btk_status btk_dual_tree_traversal_3d(btk_run_config* cfg, const btk_panel_3d* panels_target,
                                       const btk_panel_3d* panels_source, btk_interact_pair** interaction_list);
 
+/* The same interaction lists as btk_dual_tree_traversal_2d/3d (same pairs,
+ * same order, same counts in cfg), computed on the GPU one breadth-first
+ * generation of (target, source) pairs at a time. Panels are HOST arrays of
+ * the given counts (targets = sources when both pointers and counts agree);
+ * *interaction_list is a host array allocated by the library (btk_free).
+ * Synchronises the stream once per generation. No counterpart in the
+ * reference (whose traversal is host code). */
+btk_status btk_dual_tree_traversal_2d_device(btk_run_config* cfg, const btk_panel_2d* panels_target,
+                                             int target_panel_count, const btk_panel_2d* panels_source,
+                                             int source_panel_count, btk_interact_pair** interaction_list,
+                                             btk_stream_t stream);
+btk_status btk_dual_tree_traversal_3d_device(btk_run_config* cfg, const btk_panel_3d* panels_target,
+                                             int target_panel_count, const btk_panel_3d* panels_source,
+                                             int source_panel_count, btk_interact_pair** interaction_list,
+                                             btk_stream_t stream);
+
 /* src/interaction_list.cpp:252-277. Output arrays are caller storage sized by
  * the counts in the traversal's config. */
 btk_status btk_split_interactions(const btk_interact_pair* interaction_list, int interaction_count,

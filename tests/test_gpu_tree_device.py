@@ -130,3 +130,27 @@ def test_treecode_on_device_tree_solves_alike():
     oa, ob = a.solve(q).cpu().numpy(), b.solve(q).cpu().numpy()
     assert np.linalg.norm(oa - ob) <= 1e-14 * np.linalg.norm(oa)
     print(f"plan set-up: host tree {t1 - t0:.3f} s, device tree {t2 - t1:.3f} s")
+
+
+@pytest.mark.parametrize("dim,dist,n,leaf,theta,split", [(3, "uniform", 1 << 20, 2000, 0.7, False),
+                                                         (3, "plummer", 1 << 22, 2000, 0.7, False),
+                                                         (3, "sphere", 300000, 500, 0.8, False),
+                                                         (3, "mixture", 200000, 100, 0.6, True),
+                                                         (2, "uniform", 65536, 500, 0.7, False),
+                                                         (2, "uniform", 50000, 60, 0.5, True)])
+def test_device_traversal_matches_host(dim, dist, n, leaf, theta, split):
+    from barytreek_b200 import datagen
+    from barytreek_b200.treecode import (dual_tree_traversal, dual_tree_traversal_device, make_run_config,
+                                         tree_construction)
+    gen = {"uniform": lambda s, m: datagen.uniform_box(s, m, dim, -1.0, 1.0)[0],
+           "plummer": lambda s, m: datagen.plummer(s, m)[0], "sphere": lambda s, m: datagen.sphere_surface(s, m)[0],
+           "mixture": lambda s, m: datagen.gaussian_mixture(s, m)[0]}
+    cfg_h = make_run_config(dim, 6, leaf, theta, 1e-4)
+    cfg_d = make_run_config(dim, 6, leaf, theta, 1e-4)
+    tt = tree_construction(cfg_h, gen[dist](3, n))
+    ts = tree_construction(cfg_h, gen[dist](4, n // 2)) if split else None
+    host = dual_tree_traversal(cfg_h, tt, ts)
+    dev = dual_tree_traversal_device(cfg_d, tt, ts)
+    assert np.array_equal(host, dev)
+    for f in ("fmm_interaction_count", "fmm_pp_count", "fmm_pc_count", "fmm_cp_count", "fmm_cc_count"):
+        assert getattr(cfg_h, f) == getattr(cfg_d, f), f
