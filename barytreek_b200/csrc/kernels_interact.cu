@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
 // stored as PAIRS (even, odd) in packed float2 lanes, negated, so one sm_100
 // f32x2 instruction (FADD2/FMUL2/FFMA2) evaluates a target against two
 // sources: half the issue slots of scalar FP32 for the same work. Per target,
-// FP32 partial sums over kFold sources are folded into an FP64 accumulator
+// FP32 partial sums over each 256-source chunk are folded into an FP64 accumulator
 // with a compensated (two-sum) addition, so the final per-target sum carries
 // FP64 precision; the constant factor is applied in FP64 at the end.
 // ---------------------------------------------------------------------------
