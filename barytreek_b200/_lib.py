@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "libbarytreek_b200.so")
 OK, ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_UNSUPPORTED, ERR_OUT_OF_MEMORY, ERR_DEVICE_TIMEOUT, ERR_IO, ERR_INTERNAL = range(8)
 KIND_POT, KIND_VEL, KIND_FIELD = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
+DEGREE_RULE_THRESHOLD, DEGREE_RULE_COST = 0, 1
 DEGREE_FIXED, DEGREE_PER_PAIR = 0, 1
 
 # Reference struct layouts (src/structs.hpp), as numpy dtypes for host arrays.
@@ -137,6 +138,7 @@ SIGNATURES = {
     "btk_solve_host": [_ci, _ci, _ci, _ci, _ci, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_measure_pipe_peak": [_ci, _vp, _vp],
     "btk_plan_set_degrees": [_vp, _vp, _vp, _vp],
+    "btk_plan_set_degree_rule": [_vp, _ci],
     "btk_selector_param_count": [],
     "btk_selector_create": [_vp, _vp, _vp],
     "btk_selector_destroy": [_vp],

@@ -148,6 +148,9 @@ cudaError_t launch_pair_features(int n_pairs, const int* ptype, const int* ptgt,
                                  int n_points, const double4* pts, double* gsum, float* feat, cudaStream_t s);
 cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const float* feat, float* out,
                              cudaStream_t s);
+cudaError_t launch_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, const float* pred, float log10_target, int lo,
+                                       int hi, const int* pc_tcount, const int* cp_scount, const int* weight,
+                                       float inv_cbar, float inv_wbar, int* deg, cudaStream_t s);
 cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int* deg,
                                   cudaStream_t s);
 // Far-field evaluations at the chosen degrees (summed into *evals) and the

@@ -533,6 +533,9 @@ struct btk_plan {
   int n_audit = 0, n_items_main = 0, n_audit_items = 0;
   int work_split = 8;  // work items per persistent-grid slot
   double adaptive_pair_tol = 0;  // learned solves with pair_tol <= 0 (0: not yet set)
+  int degree_rule = BTK_DEGREE_RULE_COST;
+  int* d_pair_weight = nullptr;       // points under each pair's target panel
+  float inv_cbar = 1.f, inv_wbar = 1.f;  // 1 / mean pair cost at the plan degree, 1 / mean weight
   int* d_audit_orig = nullptr;
   double4* d_audit_T4 = nullptr;
   double *d_audit_out = nullptr, *d_audit_sums = nullptr;
@@ -762,6 +765,22 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     BTK_TRY(A.upload(&P->d_pair_type, ty));
     BTK_TRY(A.upload(&P->d_pair_tgt, tg));
     BTK_TRY(A.upload(&P->d_pair_src, sr));
+    // Cost-aware degree rule: each pair's weight (targets carrying its error)
+    // and the mean cost and weight that normalise its objective.
+    std::vector<int> wt(std::max(P->n_pairs, 1), 1);
+    double csum = 0, wsum = 0;
+    const double m = (double)P->degree + 1, md = dim == 3 ? m * m * m : m * m;
+    for (int i = 0; i < P->n_pairs; ++i) {
+      wt[i] = std::max(1, T.h.point_count[tg[i]]);
+      wsum += wt[i];
+      csum += i < P->n_pc ? md * P->h_pc_tcount[i]
+                          : (i < P->n_pc + P->n_cp ? md * P->h_cp_scount[i - P->n_pc] : md * md);
+    }
+    if (P->n_pairs > 0) {
+      P->inv_cbar = (float)(P->n_pairs / std::max(csum, 1.0));
+      P->inv_wbar = (float)(P->n_pairs / std::max(wsum, 1.0));
+    }
+    BTK_TRY(A.upload(&P->d_pair_weight, wt));
     std::vector<int> tc(P->h_pc_tcount), sc(P->h_cp_scount);
     tc.push_back(0);
     sc.push_back(0);
@@ -1220,7 +1239,13 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   BTK_TRY(btk_plan_pair_features(P, xs, ys, zs, charges, P->d_feat, stream));
   BTK_CUDA(launch_mlp_infer(P->n_pairs, sel->d_w, sel->norm, P->d_feat, P->d_pred, st));
   const int lo = std::max(std::max(degree_lo, P->degree_min), 1);
-  BTK_CUDA(launch_choose_degrees(P->n_pairs, P->d_pred, (float)std::log10(pair_tol), lo, P->degree, P->d_deg_pc, st));
+  if (P->degree_rule == BTK_DEGREE_RULE_COST)
+    BTK_CUDA(launch_choose_degrees_cost(P->n_pairs, P->dim, P->n_pc, P->n_cp, P->d_pred, (float)std::log10(pair_tol), lo,
+                                        P->degree, P->d_pc_tcount, P->d_cp_scount, P->d_pair_weight, P->inv_cbar,
+                                        P->inv_wbar, P->d_deg_pc, st));
+  else
+    BTK_CUDA(launch_choose_degrees(P->n_pairs, P->d_pred, (float)std::log10(pair_tol), lo, P->degree, P->d_deg_pc,
+                                   st));
   BTK_CUDA(cudaMemsetAsync(P->d_evals, 0, sizeof(unsigned long long), st));
   BTK_CUDA(cudaMemsetAsync(P->d_report, 0, sizeof(int) * kMaxNodes, st));
   BTK_CUDA(launch_far_evals(P->dim, P->n_pc, P->n_cp, P->n_far - P->n_cp, P->d_deg_pc, P->d_pc_tcount,
@@ -1399,6 +1424,14 @@ btk_status btk_plan_error_samples(btk_plan* P, const double* xt, const double* y
   BTK_CUDA(launch_error_samples(a, d_err, st));
   BTK_CUDA(cudaMemcpyAsync(log10_err, d_err, sizeof(float) * (size_t)n * n_deg, cudaMemcpyDeviceToHost, st));
   BTK_CUDA(cudaStreamSynchronize(st));
+  return BTK_OK;
+}
+
+btk_status btk_plan_set_degree_rule(btk_plan* P, int rule) {
+  BTK_CHECK(P, BTK_ERR_INVALID_ARGUMENT, "btk_plan_set_degree_rule: null plan");
+  BTK_CHECK(rule == BTK_DEGREE_RULE_THRESHOLD || rule == BTK_DEGREE_RULE_COST, BTK_ERR_INVALID_ARGUMENT,
+            "btk_plan_set_degree_rule: unknown rule");
+  P->degree_rule = rule;
   return BTK_OK;
 }
 

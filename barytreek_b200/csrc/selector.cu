@@ -326,6 +326,36 @@ __global__ void k_choose_degrees(int n, const float* pred, float log10_target, i
   deg[i] = d;
 }
 
+// Cost-aware choice: per pair the degree minimising
+//   cost(d) / cbar + (w / wbar) * (err(d) / pair_tol)^2,
+// cost(d) = evaluations at degree d ((d+1)^dim per target point for PC, per
+// source point for CP, (d+1)^(2 dim) for CC), w = points under the target
+// panel (how many targets carry the pair's error), err(d) = the predicted
+// error. The Lagrangian of "fewest evaluations for a given sum of squared
+// errors over the targets": expensive pairs accept a larger error, cheap ones
+// a smaller one, where the uniform threshold gives every pair the same.
+__global__ void k_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, const float* pred, float log10_target,
+                                      int lo, int hi, const int* pc_tcount, const int* cp_scount, const int* weight,
+                                      float inv_cbar, float inv_wbar, int* deg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float wr = (float)weight[i] * inv_wbar;
+  float best = 3.4e38f;
+  int d_best = hi;
+  for (int c = max(lo, kDegLo); c <= hi && c < kDegLo + kO; ++c) {
+    const float m = (float)(c + 1);
+    const float md = dim == 3 ? m * m * m : m * m;
+    const float cost = i < n_pc ? md * (float)pc_tcount[i] : (i < n_pc + n_cp ? md * (float)cp_scount[i - n_pc] : md * md);
+    const float e = exp10f(fminf(pred[(size_t)i * kO + (c - kDegLo)] - log10_target, 18.f));
+    const float J = cost * inv_cbar + wr * e * e;
+    if (J < best) {
+      best = J;
+      d_best = c;
+    }
+  }
+  deg[i] = d_best;
+}
+
 // Far-field evaluations at the chosen degrees (pairs PC, CP, CC in order).
 __global__ void k_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
                             const int* cp_scount, unsigned long long* evals, int* hist) {
@@ -652,6 +682,16 @@ cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, 
                                   cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   k_choose_degrees<<<(n + 255) / 256, 256, 0, s>>>(n, pred, log10_target, lo, hi, deg);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, const float* pred, float log10_target, int lo,
+                                       int hi, const int* pc_tcount, const int* cp_scount, const int* weight,
+                                       float inv_cbar, float inv_wbar, int* deg, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_choose_degrees_cost<<<(n + 255) / 256, 256, 0, s>>>(n, dim, n_pc, n_cp, pred, log10_target, lo, hi, pc_tcount,
+                                                        cp_scount, weight, inv_cbar, inv_wbar, deg);
   count_launch();
   return cudaGetLastError();
 }

