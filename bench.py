@@ -315,6 +315,20 @@ def run_native(args, world, rank, local):
         results[name]["setup_s"] = setup
     plain_evals = forms["plain"].tc.evals()
     H = results[headline]
+    # plan set-up of the headline form with the trees and lists built on the
+    # GPU (what a caller with moving points pays per rebuild), against the
+    # host-built set-up timed above
+    import barytreek_b200 as btk
+    setup_dev = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tcd = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind,
+                           precision=forms[headline].tc.precision, degree_mode=forms[headline].tc.degree_mode,
+                           degree_min=forms[headline].tc.degree_min, device_tree=True)
+        torch.cuda.synchronize()
+        setup_dev.append(time.perf_counter() - t0)
+        tcd.close()
     ms_per_step = H["ms"]
     value = world * plain_evals / (ms_per_step * 1e-3)
 
@@ -393,6 +407,8 @@ def run_native(args, world, rank, local):
         "e2e": {"value": e2e_value, "unit": "interactions/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_total / args.steps},
         "gpu_launches": H["launches"],
+        "setup": {"host_tree_s": H["setup_s"], "device_tree_s": statistics.median(setup_dev),
+                  "what": "plan creation of the headline form: tree, traversal, split, work lists, device plan"},
         "clocks": H["clocks"],
         "accuracy": {"rel_l2_vs_direct_10k": acc[headline], "per_component": per_comp},
     }
