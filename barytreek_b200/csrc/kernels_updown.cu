@@ -175,6 +175,75 @@ __global__ void __launch_bounds__(256) k_leaf_moments(const int* leaves, const i
   }
 }
 
+// 3-D base_pots with register tiles: thread (a, b) of a group of M^2 threads
+// keeps W[a][b][0..M-1]; G groups take every G-th point of a chunk and their
+// partial sums are added at the end. Per point a thread reads Lx_a q, Ly_b and
+// the M values Lz_c (shared-memory broadcasts) for M + 1 FP64 operations.
+template <int M>
+__global__ void __launch_bounds__(256) k_leaf_moments3(const int* leaves, const int* leaf_begin, const int* point_count,
+                                                       const double4* pts, const double* nodes_interp, double* psw) {
+  constexpr int IPC = M * M * M;
+  constexpr int PCH = 32;
+  constexpr int G = 256 / (M * M) > 0 ? 256 / (M * M) : 1;
+  constexpr int RED_ROWS = G > 1 ? G - 1 : 1;
+  constexpr int RED_COLS = G > 1 ? IPC : 1;
+  __shared__ double sb[3][PCH][M];
+  __shared__ double snode[3][kMaxNodes];
+  __shared__ double red[RED_ROWS][RED_COLS];
+  const int L = leaves[blockIdx.x];
+  const int b = leaf_begin[L], cnt = point_count[L];
+  const int t = threadIdx.x;
+  const int grp = t / (M * M), ab = t % (M * M);
+  const bool active = grp < G;
+  const int a = ab / M, bb = ab % M;
+  if (t < 3 * kMaxNodes) snode[t / kMaxNodes][t % kMaxNodes] = nodes_interp[(size_t)L * kPanelNodes + t];
+  double acc[M];
+#pragma unroll
+  for (int c = 0; c < M; ++c) acc[c] = 0.0;
+  __syncthreads();
+  for (int p0 = 0; p0 < cnt; p0 += PCH) {
+    if (t < PCH * 3) {
+      const int pp = t / 3, d = t % 3;
+      if (p0 + pp < cnt) {
+        const double4 pt = pts[b + p0 + pp];
+        const double x = d == 0 ? pt.x : (d == 1 ? pt.y : pt.z);
+        double Lv[M];
+        bary_basis<M>(Lv, x, snode[d]);
+        // the charge is folded into the x factor (changes only the last bit
+        // against the reference's product order, upward_pass_impl.hpp:164)
+#pragma unroll
+        for (int i = 0; i < M; ++i) sb[d][pp][i] = d == 0 ? Lv[i] * pt.w : Lv[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < M; ++i) sb[d][pp][i] = 0.0;
+      }
+    }
+    __syncthreads();
+    if (active) {
+      const int np = min(PCH, cnt - p0);
+      for (int pp = grp; pp < np; pp += G) {
+        const double v = sb[0][pp][a] * sb[1][pp][bb];
+#pragma unroll
+        for (int c = 0; c < M; ++c) acc[c] = fma(v, sb[2][pp][c], acc[c]);
+      }
+    }
+    __syncthreads();
+  }
+  if (G > 1 && active && grp > 0) {
+#pragma unroll
+    for (int c = 0; c < M; ++c) red[grp - 1][ab * M + c] = acc[c];
+  }
+  __syncthreads();
+  if (active && grp == 0) {
+#pragma unroll
+    for (int c = 0; c < M; ++c) {
+      double v = acc[c];
+      for (int g = 1; g < G; ++g) v += red[g - 1][ab * M + c];
+      psw[(size_t)L * IPC + ab * M + c] += v;
+    }
+  }
+}
+
 // Applies one 1-D factor along axis `ax` of a tensor in tensor order:
 // out[..i..] = sum_j A(i, j) in[..j..], A(i,j) = T ? X[j][i] : X[i][j].
 template <int DIM, int M, int AX, bool T>
@@ -414,8 +483,8 @@ cudaError_t launch_leaf_moments(int dim, int degree, int n_leaves, const int* le
     BTK_DISPATCH_M(degree, k_leaf_moments<2, M><<<n_leaves, 256, 0, s>>>(leaves, leaf_begin, point_count, pts,
                                                                          nodes_interp, psw));
   } else {
-    BTK_DISPATCH_M(degree, k_leaf_moments<3, M><<<n_leaves, 256, 0, s>>>(leaves, leaf_begin, point_count, pts,
-                                                                         nodes_interp, psw));
+    BTK_DISPATCH_M(degree, k_leaf_moments3<M><<<n_leaves, 256, 0, s>>>(leaves, leaf_begin, point_count, pts,
+                                                                       nodes_interp, psw));
   }
   count_launch();
   return cudaGetLastError();
