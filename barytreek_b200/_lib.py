@@ -66,7 +66,8 @@ class PlanDesc(ctypes.Structure):
 class PlanStats(ctypes.Structure):
     _fields_ = [("evals_pp", ctypes.c_int64), ("evals_pc", ctypes.c_int64), ("evals_cp", ctypes.c_int64),
                 ("evals_cc", ctypes.c_int64), ("work_items", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
-                ("levels_target", ctypes.c_int), ("levels_source", ctypes.c_int)]
+                ("levels_target", ctypes.c_int), ("levels_source", ctypes.c_int),
+                ("build_ms_total", ctypes.c_float), ("build_ms_work", ctypes.c_float)]
 
 
 class ForestDesc(ctypes.Structure):

@@ -1,10 +1,13 @@
 // Host orchestration: tree sides on the device, interaction work lists, the
 // plan API and the reference-named drop-in entry points.
 #include <algorithm>
+#include <array>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -233,34 +236,87 @@ struct WorkLists {
 // each PC pair, for re-pointing when per-pair degrees change.
 // split: work items per persistent-grid slot the cost cap aims at (longer
 // source lists are cut into atomic pieces).
+// Runs fn(begin, end) over [0, n) on up to `threads` host threads (serially
+// when the range is small).
+template <class F>
+void parallel_ranges(int64_t n, int threads, int64_t min_per_thread, F fn) {
+  const int t = (int)std::max<int64_t>(1, std::min<int64_t>(threads, n / std::max<int64_t>(1, min_per_thread)));
+  if (t <= 1) {
+    fn((int64_t)0, n, 0);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int k = 1; k < t; ++k) pool.emplace_back(fn, n * k / t, n * (k + 1) / t, k);
+  fn((int64_t)0, n / t, 0);
+  for (auto& th : pool) th.join();
+}
+
+int host_threads() {
+  static const int n = std::max(1, std::min(32, (int)std::thread::hardware_concurrency()));
+  return n;
+}
+
 btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* const lists[4], const int counts[4],
                       int grid_slots, WorkLists& W, const std::vector<long long>* pc_begin = nullptr,
                       std::vector<int>* pc_entry = nullptr, int split = 8) {
   const int ipc = S.ipc;
   const int nt = T.n_points, ns = S.n_points;
   const int Pt = T.h.panel_count, Ps = S.h.panel_count;
-  // Stable grouping of pairs by target panel: point targets take PP then PC
-  // pairs, proxy targets CP then CC, each in list order.
+  // The four lists as one sequence (PP, PC, CP, CC, each in list order),
+  // cut into chunks that host threads take in order.
+  const int64_t off1 = counts[0], off2 = off1 + counts[1], off3 = off2 + counts[2], npairs = off3 + counts[3];
+  auto pair_at = [&](int64_t g, int& t, int& i) {
+    t = g < off1 ? 0 : (g < off2 ? 1 : (g < off3 ? 2 : 3));
+    i = (int)(g - (t == 0 ? 0 : t == 1 ? off1 : t == 2 ? off2 : off3));
+  };
+  const int nthreads = host_threads();
+  const int nchunk = (int)std::max<int64_t>(1, std::min<int64_t>(nthreads, npairs / 65536));
+  auto chunk_lo = [&](int c) { return npairs * c / nchunk; };
+  // Pass 1: validation and, per chunk, pairs per target panel.
+  std::vector<std::vector<int>> hist(nchunk, std::vector<int>(Pt, 0));
+  std::vector<int> bad(nchunk, 0);
+  parallel_ranges(nchunk, nthreads, 1, [&](int64_t cb, int64_t ce, int) {
+    for (int64_t c = cb; c < ce; ++c)
+      for (int64_t g = chunk_lo((int)c); g < chunk_lo((int)c + 1); ++g) {
+        int t, i;
+        pair_at(g, t, i);
+        const btk_interact_pair& pr = lists[t][i];
+        if (!(pr.target_panel >= 0 && pr.target_panel < Pt && pr.source_panel >= 0 && pr.source_panel < Ps)) {
+          bad[c] = 1;
+          break;
+        }
+        const bool tgt_cluster = t >= 2, src_cluster = (t & 1) != 0;
+        if (!(tgt_cluster == !T.h.is_leaf[pr.target_panel] && src_cluster == !S.h.is_leaf[pr.source_panel])) {
+          bad[c] = 2;
+          break;
+        }
+        hist[c][pr.target_panel]++;
+      }
+  });
+  for (int c = 0; c < nchunk; ++c) {
+    BTK_CHECK(bad[c] != 1, BTK_ERR_INVALID_ARGUMENT, "interaction list: panel index out of range");
+    BTK_CHECK(bad[c] != 2, BTK_ERR_INVALID_ARGUMENT,
+              "interaction list: pair type does not match the panels (PP/PC targets and PP/CP sources must be "
+              "leaves, the others non-leaf)");
+  }
+  // Stable grouping by target panel: point targets take PP then PC pairs,
+  // proxy targets CP then CC, each in list order. Chunk c writes target tp's
+  // pairs from head[tp] + (pairs of tp in chunks before c).
   std::vector<int> head(Pt + 1, 0);
-  for (int t = 0; t < 4; ++t)
-    for (int i = 0; i < counts[t]; ++i) {
-      const btk_interact_pair& pr = lists[t][i];
-      BTK_CHECK(pr.target_panel >= 0 && pr.target_panel < Pt && pr.source_panel >= 0 && pr.source_panel < Ps,
-                BTK_ERR_INVALID_ARGUMENT, "interaction list: panel index out of range");
-      const bool tgt_cluster = t >= 2, src_cluster = (t & 1) != 0;
-      BTK_CHECK(tgt_cluster == !T.h.is_leaf[pr.target_panel] && src_cluster == !S.h.is_leaf[pr.source_panel],
-                BTK_ERR_INVALID_ARGUMENT,
-                "interaction list: pair type does not match the panels (PP/PC targets and PP/CP sources must be "
-                "leaves, the others non-leaf)");
-      head[pr.target_panel + 1]++;
+  for (int tp = 0; tp < Pt; ++tp) {
+    int acc = 0;
+    for (int c = 0; c < nchunk; ++c) {
+      const int h = hist[c][tp];
+      hist[c][tp] = acc;  // now the chunk's offset within tp's group
+      acc += h;
     }
-  for (int i = 0; i < Pt; ++i) head[i + 1] += head[i];
+    head[tp + 1] = head[tp] + acc;
+  }
   std::vector<Entry> grouped(head[Pt]);
-  std::vector<int> cur(head.begin(), head.end() - 1);
-  std::vector<int> n_near(Pt, 0);  // PP entries lead each target's group
   std::vector<char> touching(head[Pt], 0);
   std::vector<int> final_index(head[Pt], -1);
-  if (pc_entry) pc_entry->assign(counts[1], -1);
+  std::vector<int> grouped_of_pc;
+  if (pc_entry) grouped_of_pc.assign(counts[1], -1);
   // A PP source leaf "touches" the target leaf when the gap between the boxes
   // is under half the target's smallest side. Only such pairs can be far
   // closer than their distance to the item's centre, so only their sources
@@ -274,105 +330,175 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
     }
     return gap <= 0.5 * side;
   };
-  for (int t = 0; t < 4; ++t)
-    for (int i = 0; i < counts[t]; ++i) {
-      const btk_interact_pair& pr = lists[t][i];
-      const int sp = pr.source_panel, tp = pr.target_panel;
-      if (t == 0) {
-        n_near[tp]++;
-        touching[cur[tp]] = touches(tp, sp);
+  std::vector<std::array<int64_t, 4>> evals_part(nchunk, std::array<int64_t, 4>{0, 0, 0, 0});
+  parallel_ranges(nchunk, nthreads, 1, [&](int64_t cb, int64_t ce, int) {
+    for (int64_t c = cb; c < ce; ++c) {
+      std::vector<int>& cur = hist[c];
+      for (int64_t g = chunk_lo((int)c); g < chunk_lo((int)c + 1); ++g) {
+        int t, i;
+        pair_at(g, t, i);
+        const btk_interact_pair& pr = lists[t][i];
+        const int sp = pr.source_panel, tp = pr.target_panel;
+        const int pos = head[tp] + cur[tp]++;
+        if (t == 0) touching[pos] = touches(tp, sp);
+        Entry e;
+        if (t & 1) {  // cluster source: its proxies
+          e.s_begin = (t == 1 && pc_begin) ? (int)(*pc_begin)[i] : ns + S.cluster_slot[sp] * ipc;
+          e.s_count = ipc;
+        } else {
+          e.s_begin = S.leaf_begin[sp];
+          e.s_count = S.h.point_count[sp];
+        }
+        const int64_t nt_pts = (t >= 2) ? ipc : T.h.point_count[tp];
+        evals_part[c][t] += nt_pts * (int64_t)e.s_count;
+        if (t == 1 && pc_entry) grouped_of_pc[i] = pos;
+        grouped[pos] = e;
       }
-      Entry e;
-      if (t & 1) {  // cluster source: its proxies
-        e.s_begin = (t == 1 && pc_begin) ? (int)(*pc_begin)[i] : ns + S.cluster_slot[sp] * ipc;
-        e.s_count = ipc;
-      } else {
-        e.s_begin = S.leaf_begin[sp];
-        e.s_count = S.h.point_count[sp];
-      }
-      const int64_t nt_pts = (t >= 2) ? ipc : T.h.point_count[tp];
-      W.evals[t] += nt_pts * (int64_t)e.s_count;
-      if (t == 1 && pc_entry) (*pc_entry)[i] = cur[tp];  // grouped position; remapped below
-      grouped[cur[tp]++] = e;
     }
+  });
+  for (int c = 0; c < nchunk; ++c)
+    for (int t = 0; t < 4; ++t) W.evals[t] += evals_part[c][t];
+  // PP pairs lead every point target's group; count them per target.
+  std::vector<int> n_near(Pt, 0);
+  for (int i = 0; i < counts[0]; ++i) n_near[lists[0][i].target_panel]++;
   // Tiles and items.
   int64_t total_cost = W.evals[0] + W.evals[1] + W.evals[2] + W.evals[3];
   const int64_t max_cost =
       std::max<int64_t>((int64_t)kTile * 8192, total_cost / std::max<int64_t>(1, (int64_t)grid_slots * split));
-  std::vector<std::pair<int64_t, WorkItem>> items;
-  for (int tp = 0; tp < Pt; ++tp) {
-    const int eb = head[tp], ee = head[tp + 1];
-    if (eb == ee) continue;
-    const int e0 = (int)W.entries.size();
-    // Touching PP sources first (stable), then the other PP sources, then PC.
-    int n_touch = 0;
-    {
-      std::vector<Entry> seg;
-      seg.reserve(n_near[tp]);
+  // Pass A per target: touching PP sources first (stable), then the other PP
+  // sources, then the rest; count its non-empty entries and its items.
+  std::vector<int> n_ent(Pt + 1, 0), n_itm(Pt + 1, 0), n_touch(Pt, 0), s_tot(Pt, 0);
+  parallel_ranges(Pt, nthreads, 256, [&](int64_t pb, int64_t pe, int) {
+    std::vector<Entry> seg;
+    for (int64_t tp = pb; tp < pe; ++tp) {
+      const int eb = head[tp], ee = head[tp + 1];
+      if (eb == ee) continue;
+      seg.clear();
       for (int k = eb; k < eb + n_near[tp]; ++k)
         if (touching[k]) seg.push_back(grouped[k]);
-      n_touch = (int)seg.size();
+      n_touch[tp] = (int)seg.size();
       for (int k = eb; k < eb + n_near[tp]; ++k)
         if (!touching[k]) seg.push_back(grouped[k]);
       std::copy(seg.begin(), seg.end(), grouped.begin() + eb);
+      int ne = 0, st = 0;
+      for (int k = eb; k < ee; ++k)
+        if (grouped[k].s_count > 0) {
+          ++ne;
+          st += grouped[k].s_count;
+        }
+      n_ent[tp] = ne;
+      s_tot[tp] = st;
+      if (st == 0) continue;
+      const bool proxy = !T.h.is_leaf[tp];
+      const int tn = proxy ? ipc : T.h.point_count[tp];
+      int ni = 0;
+      for (int a = 0; a < tn; a += kTile) {
+        const int tc = std::min(kTile, tn - a);
+        const int64_t cost = (int64_t)tc * st;
+        const int nsplit = (int)std::min<int64_t>((cost + max_cost - 1) / max_cost, ne);
+        if (nsplit <= 1) {
+          ++ni;
+          continue;
+        }
+        const int64_t per = (st + nsplit - 1) / nsplit;
+        int k = eb, acc = 0;  // walk the non-empty entries like pass B
+        bool open = false;
+        int64_t piece = 0;
+        for (; k < ee; ++k) {
+          const int sc = grouped[k].s_count;
+          if (sc <= 0) continue;
+          if (open && piece + sc > per) {
+            ++acc;
+            piece = 0;
+          }
+          piece += sc;
+          open = true;
+        }
+        if (open) ++acc;
+        ni += acc;
+      }
+      n_itm[tp] = ni;
     }
-    int s_total = 0, e_near = e0;
-    for (int k = eb; k < ee; ++k) {
-      if (grouped[k].s_count > 0) {
-        final_index[k] = (int)W.entries.size();
-        W.entries.push_back(grouped[k]);
-        s_total += grouped[k].s_count;
+  });
+  // Offsets.
+  std::vector<int64_t> ent_off(Pt + 1, 0), itm_off(Pt + 1, 0);
+  for (int tp = 0; tp < Pt; ++tp) {
+    ent_off[tp + 1] = ent_off[tp] + n_ent[tp];
+    itm_off[tp + 1] = itm_off[tp] + n_itm[tp];
+  }
+  BTK_CHECK(ent_off[Pt] < (1ll << 31), BTK_ERR_UNSUPPORTED, "work lists: more than 2^31 entries");
+  W.entries.resize(ent_off[Pt]);
+  std::vector<std::pair<int64_t, WorkItem>> items(itm_off[Pt]);
+  // Pass B per target: entries and items at the offsets.
+  parallel_ranges(Pt, nthreads, 256, [&](int64_t pb, int64_t pe, int) {
+    for (int64_t tp = pb; tp < pe; ++tp) {
+      const int eb = head[tp], ee = head[tp + 1];
+      if (eb == ee) continue;
+      const int e0 = (int)ent_off[tp];
+      int e = e0, e_near = e0;
+      for (int k = eb; k < ee; ++k) {
+        if (grouped[k].s_count > 0) {
+          final_index[k] = e;
+          W.entries[e++] = grouped[k];
+        }
+        if (k - eb < n_touch[tp]) e_near = e;
       }
-      if (k - eb < n_touch) e_near = (int)W.entries.size();
+      const int e1 = e;
+      const int s_total = s_tot[tp];
+      if (s_total == 0) continue;
+      // Sources of entries [kb, ke) that are near-field (PP) points.
+      auto near_of = [&](int kb, int ke) {
+        int n = 0;
+        for (int k = kb; k < std::min(ke, e_near); ++k) n += W.entries[k].s_count;
+        return n;
+      };
+      const bool proxy = !T.h.is_leaf[tp];
+      const int t0 = proxy ? nt + T.cluster_slot[tp] * ipc : T.leaf_begin[tp];
+      const int tn = proxy ? ipc : T.h.point_count[tp];
+      // Origin for relative coordinates (mixed precision): the target panel's centre.
+      const PanelGeom& g = T.h.geom[tp];
+      const double c[3] = {0.5 * (g.lo[0] + g.hi[0]), 0.5 * (g.lo[1] + g.hi[1]), 0.5 * (g.lo[2] + g.hi[2])};
+      auto item = [&](int tb, int tc, int kb, int ke, int st, int flags) {
+        WorkItem w{};
+        w.t_begin = tb;
+        w.t_count = tc;
+        w.e_begin = kb;
+        w.e_end = ke;
+        w.s_total = st;
+        w.flags = flags;
+        w.near_total = near_of(kb, ke);
+        w.cx = c[0];
+        w.cy = c[1];
+        w.cz = c[2];
+        return w;
+      };
+      int64_t out = itm_off[tp];
+      for (int a = 0; a < tn; a += kTile) {
+        const int tc = std::min(kTile, tn - a);
+        const int64_t cost = (int64_t)tc * s_total;
+        const int nsplit = (int)std::min<int64_t>((cost + max_cost - 1) / max_cost, e1 - e0);
+        if (nsplit <= 1) {
+          items[out++] = {cost, item(t0 + a, tc, e0, e1, s_total, proxy ? kItemProxyTargets : 0)};
+          continue;
+        }
+        // Split the entry range into nsplit pieces of similar source counts.
+        const int64_t per = (s_total + nsplit - 1) / nsplit;
+        int k = e0;
+        while (k < e1) {
+          int kb = k, st = 0;
+          while (k < e1 && (st == 0 || st + W.entries[k].s_count <= per)) st += W.entries[k++].s_count;
+          items[out++] = {(int64_t)tc * st, item(t0 + a, tc, kb, k, st, (proxy ? kItemProxyTargets : 0) | kItemAtomic)};
+        }
+      }
     }
-    const int e1 = (int)W.entries.size();
-    // Sources of entries [kb, ke) that are near-field (PP) points.
-    auto near_of = [&](int kb, int ke) {
-      int n = 0;
-      for (int k = kb; k < std::min(ke, e_near); ++k) n += W.entries[k].s_count;
-      return n;
-    };
-    if (s_total == 0) continue;
-    const bool proxy = !T.h.is_leaf[tp];
-    const int t0 = proxy ? nt + T.cluster_slot[tp] * ipc : T.leaf_begin[tp];
-    const int tn = proxy ? ipc : T.h.point_count[tp];
-    // Origin for relative coordinates (mixed precision): the target panel's centre.
-    const PanelGeom& g = T.h.geom[tp];
-    const double c[3] = {0.5 * (g.lo[0] + g.hi[0]), 0.5 * (g.lo[1] + g.hi[1]), 0.5 * (g.lo[2] + g.hi[2])};
-    auto item = [&](int tb, int tc, int kb, int ke, int st, int flags) {
-      WorkItem w{};
-      w.t_begin = tb;
-      w.t_count = tc;
-      w.e_begin = kb;
-      w.e_end = ke;
-      w.s_total = st;
-      w.flags = flags;
-      w.near_total = near_of(kb, ke);
-      w.cx = c[0];
-      w.cy = c[1];
-      w.cz = c[2];
-      return w;
-    };
-    for (int a = 0; a < tn; a += kTile) {
-      const int tc = std::min(kTile, tn - a);
-      const int64_t cost = (int64_t)tc * s_total;
-      const int nsplit = (int)std::min<int64_t>((cost + max_cost - 1) / max_cost, e1 - e0);
-      if (nsplit <= 1) {
-        items.push_back({cost, item(t0 + a, tc, e0, e1, s_total, proxy ? kItemProxyTargets : 0)});
-        continue;
-      }
-      // Split the entry range into nsplit pieces of similar source counts.
-      const int64_t per = (s_total + nsplit - 1) / nsplit;
-      int k = e0;
-      while (k < e1) {
-        int kb = k, st = 0;
-        while (k < e1 && (st == 0 || st + W.entries[k].s_count <= per)) st += W.entries[k++].s_count;
-        items.push_back({(int64_t)tc * st, item(t0 + a, tc, kb, k, st, (proxy ? kItemProxyTargets : 0) | kItemAtomic)});
-      }
+  });
+  if (pc_entry) {
+    pc_entry->assign(counts[1], -1);
+    for (int i = 0; i < counts[1]; ++i) {
+      const int k = grouped_of_pc[i];
+      (*pc_entry)[i] = k >= 0 ? final_index[k] : -1;
     }
   }
-  if (pc_entry)
-    for (int& k : *pc_entry) k = k >= 0 ? final_index[k] : -1;
   std::stable_sort(items.begin(), items.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
   W.items.resize(items.size());
   for (size_t i = 0; i < items.size(); ++i) W.items[i] = items[i].second;
@@ -533,6 +659,7 @@ struct btk_plan {
   int n_audit = 0, n_items_main = 0, n_audit_items = 0;
   int work_split = 8;  // work items per persistent-grid slot
   double adaptive_pair_tol = 0;  // learned solves with pair_tol <= 0 (0: not yet set)
+  float build_ms_total = 0, build_ms_work = 0;  // host time of plan creation, of which work lists
   int degree_rule = BTK_DEGREE_RULE_COST;
   int* d_pair_weight = nullptr;       // points under each pair's target panel
   float inv_cbar = 1.f, inv_wbar = 1.f;  // 1 / mean pair cost at the plan degree, 1 / mean weight
@@ -680,7 +807,11 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   const int counts_static[4] = {counts[0], counts[1], 0, 0};
   WorkLists W;
   std::vector<int> pc_entry;
-  BTK_TRY(build_work(T, S, lists, counts_static, slots, W, &pc_begin, &pc_entry, P->work_split));
+  {
+    const auto t0 = std::chrono::steady_clock::now();
+    BTK_TRY(build_work(T, S, lists, counts_static, slots, W, &pc_begin, &pc_entry, P->work_split));
+    P->build_ms_work += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
   P->evals[0] = W.evals[0];
   P->n_static_items = (int)W.items.size();
   P->n_static_entries = (int)W.entries.size();
@@ -893,7 +1024,9 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
 
   if (D->degree_mode == BTK_DEGREE_FIXED) {
     WorkLists W;
+    const auto t0 = std::chrono::steady_clock::now();
     BTK_TRY(build_work(T, S, lists, counts, slots, W, nullptr, nullptr, P->work_split));
+    P->build_ms_work += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     for (int t = 0; t < 4; ++t) P->evals[t] = W.evals[t];
     P->ictx.n_items = (int)W.items.size();
     BTK_TRY(A.upload(&P->ictx.d_items, W.items));
@@ -940,11 +1073,13 @@ btk_status btk_plan_create(btk_plan** plan, const btk_plan_desc* desc, btk_strea
   BTK_CHECK(plan && desc, BTK_ERR_INVALID_ARGUMENT, "btk_plan_create: null argument");
   *plan = nullptr;
   btk_plan* P = new btk_plan();
+  const auto t0 = std::chrono::steady_clock::now();
   btk_status s = plan_build(P, desc, (cudaStream_t)stream);
   if (s != BTK_OK) {
     btk_plan_destroy(P);
     return s;
   }
+  P->build_ms_total = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
   *plan = P;
   return BTK_OK;
 }
@@ -970,6 +1105,8 @@ btk_status btk_plan_stats_get(const btk_plan* plan, btk_plan_stats* st) {
   st->device_bytes = (int64_t)plan->arena->bytes;
   st->levels_target = plan->tgt.h.levels;
   st->levels_source = plan->src->h.levels;
+  st->build_ms_total = plan->build_ms_total;
+  st->build_ms_work = plan->build_ms_work;
   return BTK_OK;
 }
 

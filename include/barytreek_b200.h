@@ -346,6 +346,8 @@ typedef struct {
   int64_t work_items;                             /* interaction work items */
   int64_t device_bytes;                           /* device memory the plan holds */
   int levels_target, levels_source;
+  float build_ms_total; /* host wall time of btk_plan_create */
+  float build_ms_work;  /* of which the work-list builder (grouping, near/far split, items) */
 } btk_plan_stats;
 btk_status btk_plan_stats_get(const btk_plan* plan, btk_plan_stats* stats);
 
