@@ -60,14 +60,15 @@ class PlanDesc(ctypes.Structure):
                 ("point_leaf_panel_source", ctypes.c_void_p), ("pp_list", ctypes.c_void_p),
                 ("pc_list", ctypes.c_void_p), ("cp_list", ctypes.c_void_p), ("cc_list", ctypes.c_void_p),
                 ("kind", ctypes.c_int), ("precision", ctypes.c_int), ("degree_mode", ctypes.c_int),
-                ("degree_min", ctypes.c_int), ("work_split", ctypes.c_int)]
+                ("degree_min", ctypes.c_int), ("work_split", ctypes.c_int), ("cc_operators", ctypes.c_int)]
 
 
 class PlanStats(ctypes.Structure):
     _fields_ = [("evals_pp", ctypes.c_int64), ("evals_pc", ctypes.c_int64), ("evals_cp", ctypes.c_int64),
                 ("evals_cc", ctypes.c_int64), ("work_items", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
                 ("levels_target", ctypes.c_int), ("levels_source", ctypes.c_int),
-                ("build_ms_total", ctypes.c_float), ("build_ms_work", ctypes.c_float)]
+                ("build_ms_total", ctypes.c_float), ("build_ms_work", ctypes.c_float), ("cc_groups", ctypes.c_int),
+                ("cc_tasks", ctypes.c_int)]
 
 
 class ForestDesc(ctypes.Structure):
@@ -134,6 +135,7 @@ SIGNATURES = {
     "btk_plan_create": [_vp, ctypes.POINTER(PlanDesc), _vp],
     "btk_plan_destroy": [_vp],
     "btk_plan_stats_get": [_vp, ctypes.POINTER(PlanStats)],
+    "btk_cc_operator_groups": [_ci, _vp, _ci, _vp, _ci, _vp, _ci, _vp, _vp],
     "btk_plan_execute": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_plan_last_timing": [_vp, _vp],
     "btk_solve_host": [_ci, _ci, _ci, _ci, _ci, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp],

@@ -25,7 +25,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.pat
 PER_FILE = {"host_tree.cpp": ["-Xcompiler", "-ffp-contract=off"], "tree_device.cu": ["-Xcompiler", "-ffp-contract=off"],
             "traverse_device.cu": ["-Xcompiler", "-ffp-contract=off"]}
 SOURCES = ["host_tree.cpp", "plan.cu", "kernels_updown.cu", "kernels_interact.cu", "kernels_direct.cu",
-           "kernels_probe.cu", "kernels_degree.cu", "selector.cu", "direct_noalloc.cu", "batch.cpp", "tree_device.cu", "traverse_device.cu"]
+           "kernels_probe.cu", "kernels_degree.cu", "selector.cu", "direct_noalloc.cu", "batch.cpp", "tree_device.cu", "traverse_device.cu",
+           "cc_operators.cu"]
 HEADERS = ["btk_internal.h", "kernels.cuh", "device_math.cuh"]
 
 

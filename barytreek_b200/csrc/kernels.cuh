@@ -108,6 +108,35 @@ int interact_blocks_per_sm(int dim, int kind, int precision, bool guard);
 cudaError_t launch_direct(int dim, int kind, double eps, int nt, const double* xt, const double* yt,
                           const double* zt, int ns, const double4* src, double* out, cudaStream_t s);
 
+// ---- CC pairs as shared kernel matrices (cc_operators.cu) ---------------------
+struct CcTask {
+  int tp, sp;            // the group's first pair: its panels give G's geometry
+  int p_begin, p_count;  // pairs [p_begin, p_begin + p_count) of the pair array
+};
+struct CcPair {
+  int t_row, s_row;  // target panel (row of the proxy target weights), source panel (row of psw)
+};
+struct CcParams {
+  const CcTask* tasks;
+  const CcPair* pairs;
+  const double* nodes_t;  // target side nodes_shift
+  const double* nodes_s;  // source side nodes_shift
+  const double* psw;      // [source panels][ipc]
+  Ptr4 ptw;               // per component [target panels][ipc]
+  double eps2;
+  double scale[4];
+  int m, ipc;
+};
+int cc_pairs_per_task(int dim, int kind);
+// f32: G and the products in FP32 (partial sums per source slab folded into
+// FP64), for mixed-precision plans; otherwise FP64 throughout.
+cudaError_t launch_cc_groups(int dim, int kind, bool guard, bool f32, const CcParams& p, const int* bucket_end,
+                             cudaStream_t s);
+bool cc_group_pairs(const HostTree& T, const HostTree& S, const btk_interact_pair* cc, int n_cc,
+                    std::vector<int>& group_of, int& n_groups);
+void cc_build_tasks(const btk_interact_pair* cc, int n_cc, const std::vector<int>& group_of, int n_groups, int pt,
+                    std::vector<CcTask>& tasks, std::vector<CcPair>& pairs, int bucket_end[3]);
+
 // ---- learned selector (selector.cu) -------------------------------------------
 // Inputs of the training-sample generator (see btk_plan_error_samples).
 struct SampleArgs {

@@ -658,6 +658,10 @@ struct btk_plan {
   // work items follow the solve's in ictx.d_items, [n_items_main, + n_audit_items)
   int n_audit = 0, n_items_main = 0, n_audit_items = 0;
   int work_split = 8;  // work items per persistent-grid slot
+  // CC pairs as shared kernel matrices (fixed-degree plans, cc_operators = 1)
+  int n_cc_groups = 0, n_cc_tasks = 0, cc_bucket_end[3] = {0, 0, 0};
+  btk::CcTask* d_cc_tasks = nullptr;
+  btk::CcPair* d_cc_pairs = nullptr;
   double adaptive_pair_tol = 0;  // learned solves with pair_tol <= 0 (0: not yet set)
   float build_ms_total = 0, build_ms_work = 0;  // host time of plan creation, of which work lists
   int degree_rule = BTK_DEGREE_RULE_COST;
@@ -1025,9 +1029,32 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
   if (D->degree_mode == BTK_DEGREE_FIXED) {
     WorkLists W;
     const auto t0 = std::chrono::steady_clock::now();
-    BTK_TRY(build_work(T, S, lists, counts, slots, W, nullptr, nullptr, P->work_split));
+    // CC pairs grouped by geometry leave the pairwise work lists.
+    int counts_w[4] = {counts[0], counts[1], counts[2], counts[3]};
+    if (D->cc_operators && counts[3] > 0) {
+      std::vector<int> group_of;
+      int ng = 0;
+      if (cc_group_pairs(T.h, S.h, lists[3], counts[3], group_of, ng)) {
+        for (int i = 0; i < counts[3]; ++i) {
+          const btk_interact_pair& pr = lists[3][i];
+          BTK_CHECK(!T.h.is_leaf[pr.target_panel] && !S.h.is_leaf[pr.source_panel], BTK_ERR_INVALID_ARGUMENT,
+                    "interaction list: CC pair with a leaf panel");
+        }
+        std::vector<CcTask> tasks;
+        std::vector<CcPair> pairs;
+        cc_build_tasks(lists[3], counts[3], group_of, ng, cc_pairs_per_task(P->dim, P->kind), tasks, pairs,
+                       P->cc_bucket_end);
+        BTK_TRY(A.upload(&P->d_cc_tasks, tasks));
+        BTK_TRY(A.upload(&P->d_cc_pairs, pairs));
+        P->n_cc_groups = ng;
+        P->n_cc_tasks = (int)tasks.size();
+        counts_w[3] = 0;
+      }
+    }
+    BTK_TRY(build_work(T, S, lists, counts_w, slots, W, nullptr, nullptr, P->work_split));
     P->build_ms_work += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     for (int t = 0; t < 4; ++t) P->evals[t] = W.evals[t];
+    if (P->n_cc_tasks > 0) P->evals[3] = (int64_t)counts[3] * P->ipc * P->ipc;
     P->ictx.n_items = (int)W.items.size();
     BTK_TRY(A.upload(&P->ictx.d_items, W.items));
     BTK_TRY(A.upload(&P->ictx.d_entries, W.entries));
@@ -1107,6 +1134,8 @@ btk_status btk_plan_stats_get(const btk_plan* plan, btk_plan_stats* st) {
   st->levels_source = plan->src->h.levels;
   st->build_ms_total = plan->build_ms_total;
   st->build_ms_work = plan->build_ms_work;
+  st->cc_groups = plan->n_cc_groups;
+  st->cc_tasks = plan->n_cc_tasks;
   return BTK_OK;
 }
 
@@ -1156,6 +1185,21 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
   BTK_CUDA(cudaEventRecord(P->ev[4], st));
   BTK_CUDA(cudaEventRecord(P->ev[5], st));
   BTK_TRY(run_interactions(P->ictx, P->d_S4, P->d_T4, P->d_T_out, o, per_pair ? wm : w, st, P->ev[4], P->ev[5]));
+  if (P->n_cc_tasks > 0) {
+    CcParams cp{};
+    cp.tasks = P->d_cc_tasks;
+    cp.pairs = P->d_cc_pairs;
+    cp.nodes_t = T.d_nodes_shift;
+    cp.nodes_s = S.d_nodes_shift;
+    cp.psw = P->d_psw;
+    cp.ptw = w;
+    cp.eps2 = P->eps * P->eps;
+    kind_scales(P->dim, P->kind, cp.scale);
+    cp.m = P->m;
+    cp.ipc = P->ipc;
+    BTK_CUDA(launch_cc_groups(P->dim, P->kind, cp.eps2 < 1.1754943508222875e-38, P->precision == BTK_PREC_MIXED, cp,
+                              P->cc_bucket_end, st));
+  }
   if (per_pair)
     BTK_CUDA(launch_promote(P->dim, P->degree, P->ncomp, (int)T.clusters.size(), P->d_t_cluster_panel,
                             P->d_t_cluster_slot_begin, P->d_t_slot_deg, P->d_t_slot_off, P->d_amat, P->d_amat_off,

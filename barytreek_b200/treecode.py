@@ -18,6 +18,7 @@ from ._lib import (KIND_FIELD, KIND_POT, KIND_VEL, PAIR_DTYPE, PANEL2_DTYPE, PAN
                    RunConfig, TreeInfo, check, load, ptr)
 
 __all__ = ["make_run_config", "read_run_config", "tree_construction", "dual_tree_traversal", "split_interactions",
+           "cc_operator_groups",
            "HostTree", "Treecode", "ncomp", "KIND_POT", "KIND_VEL", "KIND_FIELD", "PREC_FP64", "PREC_MIXED"]
 
 
@@ -206,26 +207,43 @@ def split_interactions(cfg: RunConfig, interactions: np.ndarray):
     return tuple(lists)
 
 
+def cc_operator_groups(dim: int, target: HostTree, cc_list: np.ndarray, source: HostTree | None = None):
+    """Group id of every CC pair under the shared-matrix CC form (host only):
+    pairs with equal target level, source level and lattice offset share one.
+    Returns (group_of_pair int32[n_cc], n_groups); n_groups is 0 (ids -1) when
+    the trees are not midpoint subdivisions of one common root box."""
+    g = np.full(len(cc_list), -1, np.int32)
+    n = ctypes.c_int(0)
+    src = source.panels if source is not None else None
+    check(load().btk_cc_operator_groups(dim, ptr(target.panels), target.panel_count, ptr(src) if src is not None else None,
+                                        source.panel_count if source is not None else 0,
+                                        ptr(cc_list) if len(cc_list) else None, len(cc_list),
+                                        ptr(g) if len(g) else None, ctypes.byref(n)))
+    return g, n.value
+
+
 class Treecode:
     """A resident treecode plan: targets = sources unless ``sources`` is given.
 
     ``coords``: tuple of dim float64 arrays (host). Trees and lists are built
     with the bit-identical host functions (``device_tree=True``: the same tree
     and lists built on the GPU from the device copies of the points), then a device plan holds the
-    leaf ordering, geometry and interaction work lists. :meth:`solve` takes
+    leaf ordering, geometry and interaction work lists. ``cc_operators=True`` applies the CC pairs of
+    a fixed-degree plan as shared kernel matrices (pairs grouped by level and lattice offset). :meth:`solve` takes
     charges (numpy or a CUDA tensor) and returns a CUDA tensor
     ``[ncomp, n_targets]`` in the original point order.
     """
 
     def __init__(self, coords, sources=None, *, degree=8, cluster_size=100, theta=0.7, eps=1e-4, kind=KIND_POT,
                  precision=PREC_FP64, degree_mode=_lib.DEGREE_FIXED, degree_min=1, work_split=0, device_tree=False,
-                 device="cuda"):
+                 cc_operators=False, device="cuda"):
         import torch
 
         self.dim = len(coords)
         self.kind, self.precision = kind, precision
         self.degree_mode, self.degree_min = degree_mode, degree_min
         self.work_split = work_split
+        self.cc_operators = bool(cc_operators)
         self.ncomp = ncomp(self.dim, kind)
         self.cfg = make_run_config(self.dim, degree, cluster_size, theta, eps)
         self.targets = tuple(np.ascontiguousarray(c, np.float64) for c in coords)
@@ -269,6 +287,7 @@ class Treecode:
         d.kind, d.precision = self.kind, self.precision
         d.degree_mode, d.degree_min = self.degree_mode, self.degree_min
         d.work_split = self.work_split
+        d.cc_operators = int(self.cc_operators)
         stream = torch.cuda.current_stream(self.device).cuda_stream
         check(load().btk_plan_create(ctypes.byref(self._plan), ctypes.byref(d), stream))
 

@@ -327,6 +327,18 @@ typedef struct {
   /* Work items per persistent-grid slot the interaction scheduler aims at
    * (source lists of costlier items are cut into pieces); 0 = 8. */
   int work_split;
+  /* 1: CC pairs are applied as shared kernel matrices (no reference
+   * counterpart; a change of evaluation order, not of the method). The boxes
+   * of one level are translates of each other, so pairs with equal target
+   * level, source level and lattice offset share the proxy-to-proxy matrix G:
+   * each such group becomes one FP64 matrix product, G evaluated once per
+   * block for up to 16 pairs (32 for the potential; btk_cc_operator_groups
+   * gives the grouping).
+   * Used by BTK_DEGREE_FIXED plans whose trees are midpoint subdivisions of
+   * one root box (one tree, or two trees over bitwise-equal root boxes);
+   * ignored otherwise (btk_plan_stats.cc_groups = 0). 0: pairwise, as the
+   * reference. */
+  int cc_operators;
 } btk_plan_desc;
 
 enum { BTK_DEGREE_FIXED = 0, BTK_DEGREE_PER_PAIR = 1 };
@@ -348,8 +360,21 @@ typedef struct {
   int levels_target, levels_source;
   float build_ms_total; /* host wall time of btk_plan_create */
   float build_ms_work;  /* of which the work-list builder (grouping, near/far split, items) */
+  int cc_groups;        /* CC pair groups applied as shared matrices (0: pairwise CC) */
+  int cc_tasks;         /* tasks of the CC-group launches (groups cut into pieces of <= 16 or 32 pairs) */
 } btk_plan_stats;
 btk_status btk_plan_stats_get(const btk_plan* plan, btk_plan_stats* stats);
+
+/* Host-only grouping behind btk_plan_desc.cc_operators: pairs of the CC list
+ * whose target level, source level and box-centre offset (in lattice units of
+ * the finest level) agree get the same group id, groups numbered in key
+ * order (target level, source level, offset x, y, z). panels_source NULL (or
+ * equal to panels_target): one tree. When the trees are not midpoint
+ * subdivisions of one common root box, *n_groups = 0 and every
+ * group_of_pair[i] = -1. Panels must be in breadth-first level order. */
+btk_status btk_cc_operator_groups(int dim, const void* panels_target, int n_target, const void* panels_source,
+                                  int n_source, const btk_interact_pair* cc_list, int n_cc, int* group_of_pair,
+                                  int* n_groups);
 
 /* One solve on device-resident inputs: gathers points and charges into leaf
  * order, runs the upward pass, the interactions and the downward pass, and
