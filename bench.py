@@ -229,7 +229,8 @@ def load_traffic(key):
 
 class Form:
     """One way of solving the workload: plain FP64 fixed degree (the reference
-    method), mixed precision fixed degree, or learned degrees + mixed."""
+    method), mixed precision fixed degree, or learned degrees + mixed; the
+    *_cc names apply the CC pairs as shared kernel matrices (cc_operators)."""
 
     def __init__(self, name, pts, args):
         import barytreek_b200 as btk
@@ -237,12 +238,12 @@ class Form:
         self.name = name
         kind = args.kind
         self.sel = None
-        if name == "plain":
+        if name in ("plain", "plain_cc"):
             self.tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind,
-                                   precision=btk.PREC_FP64)
-        elif name == "mixed":
+                                   precision=btk.PREC_FP64, cc_operators=name.endswith("_cc"))
+        elif name in ("mixed", "mixed_cc"):
             self.tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind,
-                                   precision=btk.PREC_MIXED)
+                                   precision=btk.PREC_MIXED, cc_operators=name.endswith("_cc"))
         else:
             self.tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind,
                                    precision=btk.PREC_MIXED, degree_mode=btk._lib.DEGREE_PER_PAIR, degree_min=4)
@@ -304,7 +305,8 @@ def run_native(args, world, rank, local):
     headline = args.form
     if headline == "learned" and not os.path.exists(selector.DEFAULT_WEIGHTS):
         headline = "mixed"
-    names = ["plain", "mixed", "learned"] if headline == "learned" else sorted({"plain", headline})
+    names = (["plain", "mixed", "learned", "plain_cc", "mixed_cc"] if headline == "learned"
+             else sorted({"plain", headline}))
     results, forms = {}, {}
     for name in names:
         t0 = time.time()
