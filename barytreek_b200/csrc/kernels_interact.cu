@@ -318,7 +318,7 @@ __device__ __forceinline__ void two_sum_add(double& sum, double& comp, double b)
 }
 
 template <int DIM, int KIND>
-__global__ void __launch_bounds__(kInteractThreads, 4) k_interact_mixed(InteractParams p) {
+__global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4) k_interact_mixed(InteractParams p) {
   constexpr int NC = KernelTraits<DIM, KIND>::NC;
   constexpr int TPT = kTargetsPerThread;
   static_assert(TPT == 2, "targets of a warp are [64 w, 64 w + 64): two per thread");
