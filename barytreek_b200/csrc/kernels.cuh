@@ -41,9 +41,9 @@ struct WorkItem {
   int s_total;         // sources over the entries
   int flags;           // kItemProxyTargets | kItemAtomic | kItemAudit
   int near_total;      // the first near_total sources are PP (near-field) points
-  int pad1;
-  double cx, cy, cz;   // FP64 centre of the target panel (mixed precision origin)
-  double pad2;
+  float hx;            // half widths of the target box (mixed: a near source farther than
+  double cx, cy, cz;   //   max(hx, hy, hz) from the box takes the FP32 path); FP64 centre of
+  float hy, hz;        //   the target panel (mixed precision origin)
 };
 static_assert(sizeof(WorkItem) == 64, "WorkItem is one 64-byte record");
 constexpr int kItemProxyTargets = 1;  // outputs go to proxy target weights

@@ -332,9 +332,10 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
   __shared__ __align__(8) uint64_t bars[kStages];
   __shared__ int s_item, s_abort;
   __shared__ uint32_t s_fail_chunk;
+  __shared__ int s_ncp[2][kInteractThreads / 32];  // per warp region: pairs on the hi/lo path
 
   const int tid = threadIdx.x;
-  const int lane = tid & 31, tbase = (tid >> 5) * 64;
+  const int lane = tid & 31, warp = tid >> 5, tbase = warp * 64;
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
@@ -356,6 +357,7 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
     const WorkItem w = p.items[it];
     if (w.t_count <= 0 || w.s_total <= 0) continue;  // unused tile of a per-pair-degree item block
     const int n_chunks = (w.s_total + kChunk - 1) / kChunk;
+    const float thr = fmaxf(w.hx, fmaxf(w.hy, w.hz));  // near sources at least this far from the box: FP32 path
 
     auto issue = [&](int c) {
       const int stage = (g + c) % kStages;
@@ -416,8 +418,17 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
       const int cnt = min(kChunk, w.s_total - c * kChunk);
       const int near_end = min(cnt, max(0, w.near_total - c * kChunk));  // near sources of this chunk
       const int b = c & 1;
+      // Potential kernel: a chunk with near-field sources is laid out per warp
+      // region (the 64 sources warp r converts fill pairs [32 r, 32 r + 32)):
+      // the near sources closer to the target box than max(hx, hy, hz) first,
+      // on the hi/lo path; the others after them, on the FP32 path (their
+      // separation is at least as large as a non-touching leaf's). The vector
+      // kinds keep every near source on the hi/lo path: their FP32 path is
+      // dearer, so the saving is smaller than the cost of the region loops.
+      const bool split = KIND == BTK_KIND_POT && near_end > 0;  // block-uniform
       {  // thread tid converts source pair tid into buffer b
         float hx[2], hy[2], hz[2], lx[2], ly[2], lz[2], ww[2];
+        bool close[2];
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
           const int j = 2 * tid + k;
@@ -426,6 +437,13 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
             split_rel(s.x, w.cx, hx[k], lx[k]);
             split_rel(s.y, w.cy, hy[k], ly[k]);
             split_rel(s.z, w.cz, hz[k], lz[k]);
+            if constexpr (KIND == BTK_KIND_POT) {
+              const float gap = fmaxf(fabsf(hx[k]) - w.hx,
+                                      fmaxf(fabsf(hy[k]) - w.hy, DIM == 3 ? fabsf(hz[k]) - w.hz : -3.0e38f));
+              close[k] = j < near_end && gap < thr;
+            } else {
+              close[k] = false;
+            }
             hx[k] = -hx[k];
             hy[k] = -hy[k];
             hz[k] = -hz[k];
@@ -437,12 +455,40 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
             hx[k] = hy[k] = hz[k] = kPadCoord;
             lx[k] = ly[k] = lz[k] = 0.f;
             ww[k] = 0.f;
+            close[k] = false;
           }
         }
-        fA[b][tid] = make_float4(hx[0], hx[1], hy[0], hy[1]);
-        fB[b][tid] = make_float4(hz[0], hz[1], ww[0], ww[1]);
-        fL[b][tid] = make_float4(lx[0], lx[1], ly[0], ly[1]);
-        fLz[b][tid] = make_float2(lz[0], lz[1]);
+        if (!split) {
+          fA[b][tid] = make_float4(hx[0], hx[1], hy[0], hy[1]);
+          fB[b][tid] = make_float4(hz[0], hz[1], ww[0], ww[1]);
+          fL[b][tid] = make_float4(lx[0], lx[1], ly[0], ly[1]);
+          fLz[b][tid] = make_float2(lz[0], lz[1]);
+        } else {
+          // slot q of the warp's 64: close sources in (lane, k) order, then the
+          // rest (padding last); source in slot q -> pair 32 warp + q / 2, lane q & 1
+          const unsigned m0 = __ballot_sync(0xffffffffu, close[0]), m1 = __ballot_sync(0xffffffffu, close[1]);
+          const unsigned lt = (1u << lane) - 1u;
+          const int cb = __popc(m0 & lt) + __popc(m1 & lt), n_close = __popc(m0) + __popc(m1);
+          const int fb = 2 * lane - cb;  // sources before this lane's two that are not close
+          const int q[2] = {close[0] ? cb : n_close + fb,
+                            close[1] ? cb + (close[0] ? 1 : 0) : n_close + fb + (close[0] ? 0 : 1)};
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            const int pr = warp * 32 + (q[k] >> 1), h = q[k] & 1;
+            float* a = reinterpret_cast<float*>(&fA[b][pr]);
+            float* bb = reinterpret_cast<float*>(&fB[b][pr]);
+            float* l = reinterpret_cast<float*>(&fL[b][pr]);
+            float* lzp = reinterpret_cast<float*>(&fLz[b][pr]);
+            a[h] = hx[k];
+            a[2 + h] = hy[k];
+            bb[h] = hz[k];
+            bb[2 + h] = ww[k];
+            l[h] = lx[k];
+            l[2 + h] = ly[k];
+            lzp[h] = lz[k];
+          }
+          if (lane == 0) s_ncp[b][warp] = (n_close + 1) >> 1;  // a pair with one close source takes hi/lo
+        }
       }
       // One barrier per chunk: buffer b is complete, every thread has finished
       // chunk c - 1 (so buffer b ^ 1 may be overwritten next), and the FP64
@@ -450,27 +496,56 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
       __syncthreads();
       if (s_abort) break;
       if (tid == 0 && c + kStages < n_chunks) issue(c + kStages);
-      const int np = (cnt + 1) / 2, nnp = (near_end + 1) / 2;  // a pair with one near source is near
-      for (int f0 = 0; f0 < np; f0 += kFoldPairs) {
-        const int f1 = min(np, f0 + kFoldPairs);
-        const int fn = min(f1, max(f0, nnp));
+      if (!split) {
+        const int np = (cnt + 1) / 2, nnp = (near_end + 1) / 2;  // a pair with one near source is near
+        for (int f0 = 0; f0 < np; f0 += kFoldPairs) {
+          const int f1 = min(np, f0 + kFoldPairs);
+          const int fn = min(f1, max(f0, nnp));
+          float2 part[TPT][NC];
+#pragma unroll
+          for (int u = 0; u < TPT; ++u)
+#pragma unroll
+            for (int k = 0; k < NC; ++k) part[u][k] = make_float2(0.f, 0.f);
+          if (nu == 2) {
+            pair_loop<DIM, KIND, true, 2, NC>(fA[b], fB[b], fL[b], fLz[b], f0, fn, T, e2, part);
+            pair_loop<DIM, KIND, false, 2, NC>(fA[b], fB[b], fL[b], fLz[b], fn, f1, T, e2, part);
+          } else if (nu == 1) {
+            pair_loop<DIM, KIND, true, 1, NC>(fA[b], fB[b], fL[b], fLz[b], f0, fn, T, e2, part);
+            pair_loop<DIM, KIND, false, 1, NC>(fA[b], fB[b], fL[b], fLz[b], fn, f1, T, e2, part);
+          }
+#pragma unroll
+          for (int u = 0; u < TPT; ++u)
+            if (u < nu) {
+#pragma unroll
+              for (int k = 0; k < NC; ++k)
+                two_sum_add(acc[u][k], comp[u][k], (double)(part[u][k].x + part[u][k].y));
+            }
+        }
+      } else if (nu > 0) {
+        static_assert(kFoldPairs == kPairs, "one fold per chunk");
         float2 part[TPT][NC];
 #pragma unroll
         for (int u = 0; u < TPT; ++u)
 #pragma unroll
           for (int k = 0; k < NC; ++k) part[u][k] = make_float2(0.f, 0.f);
-        if (nu == 2) {
-          pair_loop<DIM, KIND, true, 2, NC>(fA[b], fB[b], fL[b], fLz[b], f0, fn, T, e2, part);
-          pair_loop<DIM, KIND, false, 2, NC>(fA[b], fB[b], fL[b], fLz[b], fn, f1, T, e2, part);
-        } else if (nu == 1) {
-          pair_loop<DIM, KIND, true, 1, NC>(fA[b], fB[b], fL[b], fLz[b], f0, fn, T, e2, part);
-          pair_loop<DIM, KIND, false, 1, NC>(fA[b], fB[b], fL[b], fLz[b], fn, f1, T, e2, part);
+#pragma unroll 1
+        for (int r = 0; r < kInteractThreads / 32; ++r) {
+          const int p0 = r * 32, rp = (min(64, max(0, cnt - 64 * r)) + 1) / 2;  // pairs holding sources
+          const int pn = p0 + min(s_ncp[b][r], rp);
+          if (nu == 2) {
+            pair_loop<DIM, KIND, true, 2, NC>(fA[b], fB[b], fL[b], fLz[b], p0, pn, T, e2, part);
+            pair_loop<DIM, KIND, false, 2, NC>(fA[b], fB[b], fL[b], fLz[b], pn, p0 + rp, T, e2, part);
+          } else {
+            pair_loop<DIM, KIND, true, 1, NC>(fA[b], fB[b], fL[b], fLz[b], p0, pn, T, e2, part);
+            pair_loop<DIM, KIND, false, 1, NC>(fA[b], fB[b], fL[b], fLz[b], pn, p0 + rp, T, e2, part);
+          }
         }
 #pragma unroll
         for (int u = 0; u < TPT; ++u)
           if (u < nu) {
 #pragma unroll
-            for (int k = 0; k < NC; ++k) two_sum_add(acc[u][k], comp[u][k], (double)(part[u][k].x + part[u][k].y));
+            for (int k = 0; k < NC; ++k)
+              two_sum_add(acc[u][k], comp[u][k], (double)(part[u][k].x + part[u][k].y));
           }
       }
     }

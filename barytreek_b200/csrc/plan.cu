@@ -455,9 +455,12 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
       const bool proxy = !T.h.is_leaf[tp];
       const int t0 = proxy ? nt + T.cluster_slot[tp] * ipc : T.leaf_begin[tp];
       const int tn = proxy ? ipc : T.h.point_count[tp];
-      // Origin for relative coordinates (mixed precision): the target panel's centre.
+      // Origin for relative coordinates (mixed precision): the target panel's
+      // centre; its half widths bound the near-source test.
       const PanelGeom& g = T.h.geom[tp];
       const double c[3] = {0.5 * (g.lo[0] + g.hi[0]), 0.5 * (g.lo[1] + g.hi[1]), 0.5 * (g.lo[2] + g.hi[2])};
+      const float bh[3] = {(float)(0.5 * (g.hi[0] - g.lo[0])), (float)(0.5 * (g.hi[1] - g.lo[1])),
+                           T.h.dim == 3 ? (float)(0.5 * (g.hi[2] - g.lo[2])) : 0.f};
       auto item = [&](int tb, int tc, int kb, int ke, int st, int flags) {
         WorkItem w{};
         w.t_begin = tb;
@@ -470,6 +473,9 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
         w.cx = c[0];
         w.cy = c[1];
         w.cz = c[2];
+        w.hx = bh[0];
+        w.hy = bh[1];
+        w.hz = bh[2];
         return w;
       };
       int64_t out = itm_off[tp];
@@ -1310,6 +1316,10 @@ void build_audit_work(const btk_plan* P, int entry_base, AuditWork& W) {
       w.cx = c[0];
       w.cy = c[1];
       w.cz = c[2];
+      // unsorted sample (no tile box): every near source keeps the hi/lo path
+      w.hx = spatial ? (float)(0.5 * (hi[0] - lo[0])) : 3.0e38f;
+      w.hy = spatial ? (float)(0.5 * (hi[1] - lo[1])) : 3.0e38f;
+      w.hz = spatial && dim == 3 ? (float)(0.5 * (hi[2] - lo[2])) : (spatial ? 0.f : 3.0e38f);
       W.items.push_back(w);
       before += st;
     }
