@@ -60,7 +60,8 @@ class PlanDesc(ctypes.Structure):
                 ("point_leaf_panel_source", ctypes.c_void_p), ("pp_list", ctypes.c_void_p),
                 ("pc_list", ctypes.c_void_p), ("cp_list", ctypes.c_void_p), ("cc_list", ctypes.c_void_p),
                 ("kind", ctypes.c_int), ("precision", ctypes.c_int), ("degree_mode", ctypes.c_int),
-                ("degree_min", ctypes.c_int), ("work_split", ctypes.c_int), ("cc_operators", ctypes.c_int)]
+                ("degree_min", ctypes.c_int), ("work_split", ctypes.c_int), ("cc_operators", ctypes.c_int),
+                ("leaf_far_pairs", ctypes.c_int)]
 
 
 class PlanStats(ctypes.Structure):
@@ -68,7 +69,7 @@ class PlanStats(ctypes.Structure):
                 ("evals_cc", ctypes.c_int64), ("work_items", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
                 ("levels_target", ctypes.c_int), ("levels_source", ctypes.c_int),
                 ("build_ms_total", ctypes.c_float), ("build_ms_work", ctypes.c_float), ("cc_groups", ctypes.c_int),
-                ("cc_tasks", ctypes.c_int)]
+                ("cc_tasks", ctypes.c_int), ("leaf_far_pairs", ctypes.c_int)]
 
 
 class ForestDesc(ctypes.Structure):

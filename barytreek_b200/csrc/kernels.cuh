@@ -177,15 +177,21 @@ cudaError_t launch_pair_features(int n_pairs, const int* ptype, const int* ptgt,
                                  int n_points, const double4* pts, double* gsum, float* feat, cudaStream_t s);
 cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const float* feat, float* out,
                              cudaStream_t s);
-cudaError_t launch_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, const float* pred, float log10_target, int lo,
-                                       int hi, const int* pc_tcount, const int* cp_scount, const int* weight,
-                                       float inv_cbar, float inv_wbar, int* deg, cudaStream_t s);
-cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int* deg,
-                                  cudaStream_t s);
-// Far-field evaluations at the chosen degrees (summed into *evals) and the
-// histogram of the degrees (hist[0..12], added to).
+// Pairs [conv0, n_pc) of the PC block are leaf pairs that may stay direct
+// (degree 0); pc_direct[2 i], [2 i + 1]: their source leaf's first point and
+// point count.
+cudaError_t launch_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, int conv0, const float* pred,
+                                       float log10_target, int lo, int hi, const int* pc_tcount, const int* cp_scount,
+                                       const int* pc_direct, const int* weight, float inv_cbar, float inv_wbar,
+                                       int* deg, cudaStream_t s);
+cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int dim, int conv0,
+                                  int n_pc, const int* pc_direct, int* deg, cudaStream_t s);
+// Far-field evaluations at the chosen degrees (summed into evals[0]), direct
+// evaluations of the leaf pairs kept direct (evals[1]) and the histogram of
+// the degrees (hist[0..12], added to).
 cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
-                             const int* cp_scount, unsigned long long* evals, int* hist, cudaStream_t s);
+                             const int* cp_scount, const int* pc_direct, unsigned long long* evals, int* hist,
+                             cudaStream_t s);
 cudaError_t launch_audit_compare(int n, int ncomp, int nt, const int* audit_sorted, const int* perm,
                                  const double* out, const double* audit_out, double* sums, cudaStream_t s);
 cudaError_t launch_fill_int(int n, int value, int* dst, cudaStream_t s);
@@ -202,7 +208,7 @@ cudaError_t launch_promote(int dim, int n, int ncomp, int n_clusters, const int*
                            const int* cluster_slot_begin, const int* slot_degree, const long long* slot_offset,
                            const double* amat, const int* amat_off, Ptr4 ptwm, Ptr4 ptw, cudaStream_t s);
 cudaError_t launch_resolve(int dim, int n_pc, const int* pc_entry, const int* pc_src_cluster, const int* deg_pc,
-                           int n_far, int tiles_max, const int* far_type, const int* far_tgt_cluster,
+                           const int* pc_direct, int n_far, int tiles_max, const int* far_type, const int* far_tgt_cluster,
                            const int* far_src, const int* deg_far, const long long* src_slot_offset,
                            const int* cluster_slot_begin_s, const long long* tgt_slot_offset,
                            const int* cluster_slot_begin_t, int slot_d_lo, long long t4_base, long long s4_base,

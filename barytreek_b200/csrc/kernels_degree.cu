@@ -199,16 +199,23 @@ __global__ void __launch_bounds__(256) k_promote(int dim, int n, int ncomp, cons
 __device__ __forceinline__ int ipow_d(int b, int dim) { return dim == 3 ? b * b * b : b * b; }
 
 // Re-points the PC entries of point-target items at the chosen degree's slot.
+// Degree 0 (leaf pairs that may be approximated, kept direct): the source
+// leaf's points, pc_direct[2 i] (first) and [2 i + 1] (count).
 __global__ void k_resolve_pc(int dim, int n_pc, const int* pc_entry, const int* pc_src_cluster, const int* degree,
-                             const long long* src_slot_offset, const int* cluster_slot_begin_s, int slot_d_lo,
-                             long long s4_base, Entry* entries) {
+                             const int* pc_direct, const long long* src_slot_offset, const int* cluster_slot_begin_s,
+                             int slot_d_lo, long long s4_base, Entry* entries) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_pc) return;
   const int d = degree[i];
-  const int slot = cluster_slot_begin_s[pc_src_cluster[i]] + (d - slot_d_lo);
   Entry e;
-  e.s_begin = (int)(s4_base + src_slot_offset[slot]);
-  e.s_count = ipow_d(d + 1, dim);
+  if (d == 0) {
+    e.s_begin = pc_direct[2 * i];
+    e.s_count = pc_direct[2 * i + 1];
+  } else {
+    const int slot = cluster_slot_begin_s[pc_src_cluster[i]] + (d - slot_d_lo);
+    e.s_begin = (int)(s4_base + src_slot_offset[slot]);
+    e.s_count = ipow_d(d + 1, dim);
+  }
   const int k = pc_entry[i];
   if (k >= 0) entries[k] = e;
 }
@@ -299,15 +306,16 @@ cudaError_t launch_promote(int dim, int n, int ncomp, int n_clusters, const int*
 }
 
 cudaError_t launch_resolve(int dim, int n_pc, const int* pc_entry, const int* pc_src_cluster, const int* deg_pc,
-                           int n_far, int tiles_max, const int* far_type, const int* far_tgt_cluster,
+                           const int* pc_direct, int n_far, int tiles_max, const int* far_type, const int* far_tgt_cluster,
                            const int* far_src, const int* deg_far, const long long* src_slot_offset,
                            const int* cluster_slot_begin_s, const long long* tgt_slot_offset,
                            const int* cluster_slot_begin_t, int slot_d_lo, long long t4_base, long long s4_base,
                            const double* tgt_centre, int n_point_items, WorkItem* items, Entry* entries,
                            int far_item0, int far_entry0, cudaStream_t s) {
   if (n_pc > 0) {
-    k_resolve_pc<<<(n_pc + 255) / 256, 256, 0, s>>>(dim, n_pc, pc_entry, pc_src_cluster, deg_pc, src_slot_offset,
-                                                    cluster_slot_begin_s, slot_d_lo, s4_base, entries);
+    k_resolve_pc<<<(n_pc + 255) / 256, 256, 0, s>>>(dim, n_pc, pc_entry, pc_src_cluster, deg_pc, pc_direct,
+                                                    src_slot_offset, cluster_slot_begin_s, slot_d_lo, s4_base,
+                                                    entries);
     count_launch();
   }
   if (n_point_items > 0) {

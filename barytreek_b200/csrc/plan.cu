@@ -258,7 +258,7 @@ int host_threads() {
 
 btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* const lists[4], const int counts[4],
                       int grid_slots, WorkLists& W, const std::vector<long long>* pc_begin = nullptr,
-                      std::vector<int>* pc_entry = nullptr, int split = 8) {
+                      std::vector<int>* pc_entry = nullptr, int split = 8, std::vector<int>* pp_entry = nullptr) {
   const int ipc = S.ipc;
   const int nt = T.n_points, ns = S.n_points;
   const int Pt = T.h.panel_count, Ps = S.h.panel_count;
@@ -317,6 +317,8 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
   std::vector<int> final_index(head[Pt], -1);
   std::vector<int> grouped_of_pc;
   if (pc_entry) grouped_of_pc.assign(counts[1], -1);
+  std::vector<int> pp_at;  // PP pair at each grouped position (pp_entry only)
+  if (pp_entry) pp_at.assign(head[Pt], -1);
   // A PP source leaf "touches" the target leaf when the gap between the boxes
   // is under half the target's smallest side. Only such pairs can be far
   // closer than their distance to the item's centre, so only their sources
@@ -352,6 +354,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
         const int64_t nt_pts = (t >= 2) ? ipc : T.h.point_count[tp];
         evals_part[c][t] += nt_pts * (int64_t)e.s_count;
         if (t == 1 && pc_entry) grouped_of_pc[i] = pos;
+        if (t == 0 && pp_entry) pp_at[pos] = i;
         grouped[pos] = e;
       }
     }
@@ -370,16 +373,25 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
   std::vector<int> n_ent(Pt + 1, 0), n_itm(Pt + 1, 0), n_touch(Pt, 0), s_tot(Pt, 0);
   parallel_ranges(Pt, nthreads, 256, [&](int64_t pb, int64_t pe, int) {
     std::vector<Entry> seg;
+    std::vector<int> segp;
     for (int64_t tp = pb; tp < pe; ++tp) {
       const int eb = head[tp], ee = head[tp + 1];
       if (eb == ee) continue;
       seg.clear();
+      segp.clear();
       for (int k = eb; k < eb + n_near[tp]; ++k)
-        if (touching[k]) seg.push_back(grouped[k]);
+        if (touching[k]) {
+          seg.push_back(grouped[k]);
+          if (pp_entry) segp.push_back(pp_at[k]);
+        }
       n_touch[tp] = (int)seg.size();
       for (int k = eb; k < eb + n_near[tp]; ++k)
-        if (!touching[k]) seg.push_back(grouped[k]);
+        if (!touching[k]) {
+          seg.push_back(grouped[k]);
+          if (pp_entry) segp.push_back(pp_at[k]);
+        }
       std::copy(seg.begin(), seg.end(), grouped.begin() + eb);
+      if (pp_entry) std::copy(segp.begin(), segp.end(), pp_at.begin() + eb);
       int ne = 0, st = 0;
       for (int k = eb; k < ee; ++k)
         if (grouped[k].s_count > 0) {
@@ -504,6 +516,11 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
       const int k = grouped_of_pc[i];
       (*pc_entry)[i] = k >= 0 ? final_index[k] : -1;
     }
+  }
+  if (pp_entry) {  // final entry of each PP pair (-1: empty source leaf, no entry)
+    pp_entry->assign(counts[0], -1);
+    for (size_t k = 0; k < pp_at.size(); ++k)
+      if (pp_at[k] >= 0) (*pp_entry)[pp_at[k]] = final_index[k];
   }
   std::stable_sort(items.begin(), items.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
   W.items.resize(items.size());
@@ -635,6 +652,12 @@ struct btk_plan {
   // ---- per-pair degrees (degree_mode == BTK_DEGREE_PER_PAIR) ----
   int degree_mode = BTK_DEGREE_FIXED, degree_min = 0;
   int n_pc = 0, n_cp = 0, n_far = 0, tiles_max = 0, n_static_items = 0, n_static_entries = 0;
+  // Leaf pairs the degree choice may approximate (leaf_far_pairs): PC-block
+  // pairs [n_pc_list, n_pc), degree 0 = direct.
+  int leaf_far = 0, n_pc_list = 0;
+  double theta = 0.7;
+  int64_t conv_direct_total = 0;  // their direct evaluations (all included in evals[0])
+  int* d_pc_direct = nullptr;
   int n_src_slots = 0, n_tgt_slots = 0;
   long long total_src_slots = 0, total_tgt_slots = 0;
   int *d_s_slot_panel = nullptr, *d_s_slot_deg = nullptr, *d_s_cluster_slot_begin = nullptr;
@@ -718,7 +741,8 @@ void bary_row_unit(double x, int d, double* out) {
 void recount_far_evals(btk_plan* P) {
   auto sz = [&](int d) { return (int64_t)ipow(d + 1, P->dim); };
   P->evals[1] = P->evals[2] = P->evals[3] = 0;
-  for (int i = 0; i < P->n_pc; ++i) P->evals[1] += P->h_pc_tcount[i] * sz(P->h_deg_pc[i]);
+  for (int i = 0; i < P->n_pc; ++i)
+    if (P->h_deg_pc[i] > 0) P->evals[1] += P->h_pc_tcount[i] * sz(P->h_deg_pc[i]);
   for (int i = 0; i < P->n_cp; ++i) P->evals[2] += sz(P->h_deg_far[i]) * P->h_cp_scount[i];
   for (int i = P->n_cp; i < P->n_far; ++i) P->evals[3] += sz(P->h_deg_far[i]) * sz(P->h_deg_far[i]);
 }
@@ -743,15 +767,15 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   const int ncs = (int)S.clusters.size(), nct = (int)T.clusters.size();
   auto sz = [&](int d) { return (long long)ipow(d + 1, dim); };
   // Slot tables: cluster-major, degrees dlo..n.
-  auto make_slots = [&](const Side& X, std::vector<int>& panel, std::vector<int>& deg, std::vector<long long>& off,
-                        std::vector<int>& begin) {
-    const int nc = (int)X.clusters.size();
+  auto make_slots = [&](const std::vector<int>& slot_panels, std::vector<int>& panel, std::vector<int>& deg,
+                        std::vector<long long>& off, std::vector<int>& begin) {
+    const int nc = (int)slot_panels.size();
     long long o = 0;
     begin.resize(nc + 1);
     for (int c = 0; c < nc; ++c) {
       begin[c] = c * nd;
       for (int d = dlo; d <= n; ++d) {
-        panel.push_back(X.clusters[c]);
+        panel.push_back(slot_panels[c]);
         deg.push_back(d);
         off.push_back(o);
         o += sz(d);
@@ -760,10 +784,52 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     begin[nc] = nc * nd;
     return o;
   };
+  // Leaf pairs the degree choice may approximate: PP pairs that satisfy the
+  // MAC of the traversal, (r_t + r_s) / |c_t - c_s| < theta with r the
+  // panels' half diagonals (src/interaction_list.cpp:142-156), whose source
+  // leaf has more points than the proxies of degree_min. Their source leaves
+  // get degree slots after the clusters'.
+  std::vector<int> conv;                         // PP pair indices
+  std::vector<int> slot_panels_s(S.clusters);    // source panels with degree slots
+  std::vector<int> slot_of_s(S.cluster_slot);    // per source panel: its index there (-1: none)
+  if (P->leaf_far) {
+    for (int i = 0; i < counts[0]; ++i) {
+      const btk_interact_pair& pr = lists[0][i];
+      const int tp = pr.target_panel, sp = pr.source_panel;
+      BTK_CHECK(tp >= 0 && tp < T.h.panel_count && sp >= 0 && sp < S.h.panel_count, BTK_ERR_INVALID_ARGUMENT,
+                "interaction list: panel index out of range");
+      if (T.h.point_count[tp] <= 0 || S.h.point_count[sp] <= sz(dlo)) continue;
+      const PanelGeom &a = T.h.geom[tp], &b = S.h.geom[sp];
+      double d2 = 0, ra = 0, rb = 0;
+      for (int d = 0; d < dim; ++d) {
+        const double dc = 0.5 * (b.lo[d] + b.hi[d]) - 0.5 * (a.lo[d] + a.hi[d]);
+        d2 += dc * dc;
+        ra += (a.hi[d] - a.lo[d]) * (a.hi[d] - a.lo[d]);
+        rb += (b.hi[d] - b.lo[d]) * (b.hi[d] - b.lo[d]);
+      }
+      // (leaves within half the target's smallest side of each other stay
+      // direct: their entries lead the items, on the near-field path)
+      double gap = 0.0, side = 1e300;
+      for (int d = 0; d < dim; ++d) {
+        gap = std::max(gap, std::max(b.lo[d] - a.hi[d], a.lo[d] - b.hi[d]));
+        side = std::min(side, a.hi[d] - a.lo[d]);
+      }
+      const double dist = std::sqrt(d2);
+      if (dist > 0 && gap > 0.5 * side && (0.5 * std::sqrt(ra) + 0.5 * std::sqrt(rb)) / dist < P->theta)
+        conv.push_back(i);
+    }
+    for (int i : conv) {
+      const int sp = lists[0][i].source_panel;
+      if (slot_of_s[sp] < 0) {
+        slot_of_s[sp] = (int)slot_panels_s.size();
+        slot_panels_s.push_back(sp);
+      }
+    }
+  }
   std::vector<int> s_panel, s_deg, s_begin, t_panel, t_deg, t_begin;
   std::vector<long long> s_off, t_off;
-  P->total_src_slots = make_slots(S, s_panel, s_deg, s_off, s_begin);
-  P->total_tgt_slots = make_slots(T, t_panel, t_deg, t_off, t_begin);
+  P->total_src_slots = make_slots(slot_panels_s, s_panel, s_deg, s_off, s_begin);
+  P->total_tgt_slots = make_slots(T.clusters, t_panel, t_deg, t_off, t_begin);
   P->n_src_slots = (int)s_panel.size();
   P->n_tgt_slots = (int)t_panel.size();
   BTK_CHECK(S.n_points + P->total_src_slots < (1LL << 31) && T.n_points + P->total_tgt_slots < (1LL << 31),
@@ -800,28 +866,47 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   BTK_TRY(A.upload(&P->d_t_cluster_slot_begin, t_begin));
   BTK_TRY(A.upload(&P->d_t_cluster_panel, T.clusters));
 
-  // Static items: PP and PC (PC entries start at the degree-n slot).
-  P->n_pc = counts[1];
+  // Static items: PP and PC (PC entries start at the degree-n slot). The PC
+  // block of the per-pair arrays is the PC list, then the leaf pairs (their
+  // entries are the PP entries, direct until a degree is chosen).
+  P->n_pc_list = counts[1];
+  P->n_pc = counts[1] + (int)conv.size();
   P->n_cp = counts[2];
   P->n_far = counts[2] + counts[3];
-  std::vector<long long> pc_begin(P->n_pc);
-  std::vector<int> pc_src_cluster(P->n_pc);
+  std::vector<long long> pc_begin(P->n_pc_list);
+  std::vector<int> pc_src_cluster(P->n_pc), pc_direct(2 * (size_t)std::max(P->n_pc, 1), -1);
   P->h_pc_tcount.resize(P->n_pc);
-  for (int i = 0; i < P->n_pc; ++i) {
+  for (int i = 0; i < P->n_pc_list; ++i) {
     const int c = S.cluster_slot[lists[1][i].source_panel];
     BTK_CHECK(c >= 0, BTK_ERR_INVALID_ARGUMENT, "PC pair with a leaf source");
     pc_src_cluster[i] = c;
     pc_begin[i] = S.n_points + s_off[s_begin[c] + (n - dlo)];
     P->h_pc_tcount[i] = T.h.point_count[lists[1][i].target_panel];
   }
+  P->conv_direct_total = 0;
+  for (size_t k = 0; k < conv.size(); ++k) {
+    const btk_interact_pair& pr = lists[0][conv[k]];
+    const int i = P->n_pc_list + (int)k;
+    pc_src_cluster[i] = slot_of_s[pr.source_panel];
+    P->h_pc_tcount[i] = T.h.point_count[pr.target_panel];
+    pc_direct[2 * i] = S.leaf_begin[pr.source_panel];
+    pc_direct[2 * i + 1] = S.h.point_count[pr.source_panel];
+    P->conv_direct_total += (int64_t)P->h_pc_tcount[i] * pc_direct[2 * i + 1];
+  }
   const int counts_static[4] = {counts[0], counts[1], 0, 0};
   WorkLists W;
-  std::vector<int> pc_entry;
+  std::vector<int> pc_entry, pp_entry;
   {
     const auto t0 = std::chrono::steady_clock::now();
-    BTK_TRY(build_work(T, S, lists, counts_static, slots, W, &pc_begin, &pc_entry, P->work_split));
+    BTK_TRY(build_work(T, S, lists, counts_static, slots, W, &pc_begin, &pc_entry, P->work_split,
+                       conv.empty() ? nullptr : &pp_entry));
     P->build_ms_work += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
+  for (int i : conv) {
+    BTK_CHECK(pp_entry[i] >= 0, BTK_ERR_INTERNAL, "leaf pair without a work-list entry");
+    pc_entry.push_back(pp_entry[i]);
+  }
+  BTK_TRY(A.upload(&P->d_pc_direct, pc_direct));
   P->evals[0] = W.evals[0];
   P->n_static_items = (int)W.items.size();
   P->n_static_entries = (int)W.entries.size();
@@ -880,10 +965,12 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   P->n_items_main = (int)n_items;
   // Degrees in force: all at n until set.
   P->h_deg_pc.assign(P->n_pc, n);
+  std::fill(P->h_deg_pc.begin() + P->n_pc_list, P->h_deg_pc.end(), 0);  // leaf pairs: direct
   P->h_deg_far.assign(P->n_far, n);
   P->n_pairs = P->n_pc + P->n_far;
   {
     std::vector<int> all(std::max(P->n_pairs, 1), n);
+    std::fill(all.begin() + P->n_pc_list, all.begin() + P->n_pc, 0);
     BTK_TRY(A.upload(&P->d_deg_pc, all));  // one array: PC degrees, then CP, then CC
     P->d_deg_far = P->d_deg_pc + P->n_pc;
   }
@@ -892,9 +979,10 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   {
     std::vector<int> ty(std::max(P->n_pairs, 1)), tg(std::max(P->n_pairs, 1)), sr(std::max(P->n_pairs, 1));
     for (int i = 0; i < P->n_pc; ++i) {
+      const btk_interact_pair& pr = i < P->n_pc_list ? lists[1][i] : lists[0][conv[i - P->n_pc_list]];
       ty[i] = 1;
-      tg[i] = lists[1][i].target_panel;
-      sr[i] = lists[1][i].source_panel;
+      tg[i] = pr.target_panel;
+      sr[i] = pr.source_panel;
     }
     for (int i = 0; i < P->n_far; ++i) {
       const bool cp = i < P->n_cp;
@@ -930,9 +1018,9 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     BTK_TRY(A.alloc(&P->d_desc, (size_t)S.h.panel_count * 6));
     BTK_TRY(A.alloc(&P->d_feat, (size_t)std::max(P->n_pairs, 1) * 16));
     BTK_TRY(A.alloc(&P->d_pred, (size_t)std::max(P->n_pairs, 1) * 9));
-    BTK_TRY(A.alloc(&P->d_evals, 1));
+    BTK_TRY(A.alloc(&P->d_evals, 2));
     BTK_TRY(A.alloc(&P->d_gsum, 2));
-    BTK_TRY(A.upload(&P->d_cluster_slot_s, S.cluster_slot));
+    BTK_TRY(A.upload(&P->d_cluster_slot_s, slot_of_s));
     BTK_TRY(A.upload(&P->d_cluster_slot_t, T.cluster_slot));
     const PanelGeom& g = S.h.geom[0];
     double r2 = 0;
@@ -1026,6 +1114,8 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
   BTK_TRY(A.alloc(&P->d_psw, (size_t)Ps * P->ipc));
   BTK_TRY(A.alloc(&P->d_ptw, (size_t)P->ncomp * Pt * P->ipc));
   P->degree_mode = D->degree_mode;
+  P->leaf_far = D->degree_mode == BTK_DEGREE_PER_PAIR && D->leaf_far_pairs ? 1 : 0;
+  P->theta = cfg.fmm_theta;
   P->degree_min = D->degree_min;
   BTK_CHECK(D->work_split >= 0 && D->work_split <= 1024, BTK_ERR_INVALID_ARGUMENT, "work_split outside 0..1024");
   P->work_split = D->work_split > 0 ? D->work_split : 8;
@@ -1142,6 +1232,7 @@ btk_status btk_plan_stats_get(const btk_plan* plan, btk_plan_stats* st) {
   st->build_ms_work = plan->build_ms_work;
   st->cc_groups = plan->n_cc_groups;
   st->cc_tasks = plan->n_cc_tasks;
+  st->leaf_far_pairs = plan->n_pc - plan->n_pc_list;
   return BTK_OK;
 }
 
@@ -1169,7 +1260,8 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
     BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
                               S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
                               P->d_S4 + S.n_points, st));
-    BTK_CUDA(launch_resolve(P->dim, P->n_pc, P->d_pc_entry, P->d_pc_src_cluster, P->d_deg_pc, P->n_far, P->tiles_max,
+    BTK_CUDA(launch_resolve(P->dim, P->n_pc, P->d_pc_entry, P->d_pc_src_cluster, P->d_deg_pc, P->d_pc_direct,
+                            P->n_far, P->tiles_max,
                             P->d_far_type, P->d_far_tgt, P->d_far_src, P->d_deg_far, P->d_s_slot_off,
                             P->d_s_cluster_slot_begin, P->d_t_slot_off, P->d_t_cluster_slot_begin, P->degree_min,
                             T.n_points, S.n_points, P->d_tgt_centre, P->n_static_items, P->ictx.d_items,
@@ -1431,16 +1523,16 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   BTK_CUDA(launch_mlp_infer(P->n_pairs, sel->d_w, sel->norm, P->d_feat, P->d_pred, st));
   const int lo = std::max(std::max(degree_lo, P->degree_min), 1);
   if (P->degree_rule == BTK_DEGREE_RULE_COST)
-    BTK_CUDA(launch_choose_degrees_cost(P->n_pairs, P->dim, P->n_pc, P->n_cp, P->d_pred, (float)std::log10(pair_tol), lo,
-                                        P->degree, P->d_pc_tcount, P->d_cp_scount, P->d_pair_weight, P->inv_cbar,
-                                        P->inv_wbar, P->d_deg_pc, st));
+    BTK_CUDA(launch_choose_degrees_cost(P->n_pairs, P->dim, P->n_pc, P->n_cp, P->n_pc_list, P->d_pred,
+                                        (float)std::log10(pair_tol), lo, P->degree, P->d_pc_tcount, P->d_cp_scount,
+                                        P->d_pc_direct, P->d_pair_weight, P->inv_cbar, P->inv_wbar, P->d_deg_pc, st));
   else
-    BTK_CUDA(launch_choose_degrees(P->n_pairs, P->d_pred, (float)std::log10(pair_tol), lo, P->degree, P->d_deg_pc,
-                                   st));
-  BTK_CUDA(cudaMemsetAsync(P->d_evals, 0, sizeof(unsigned long long), st));
+    BTK_CUDA(launch_choose_degrees(P->n_pairs, P->d_pred, (float)std::log10(pair_tol), lo, P->degree, P->dim,
+                                   P->n_pc_list, P->n_pc, P->d_pc_direct, P->d_deg_pc, st));
+  BTK_CUDA(cudaMemsetAsync(P->d_evals, 0, 2 * sizeof(unsigned long long), st));
   BTK_CUDA(cudaMemsetAsync(P->d_report, 0, sizeof(int) * kMaxNodes, st));
   BTK_CUDA(launch_far_evals(P->dim, P->n_pc, P->n_cp, P->n_far - P->n_cp, P->d_deg_pc, P->d_pc_tcount,
-                            P->d_cp_scount, P->d_evals, P->d_report, st));
+                            P->d_cp_scount, P->d_pc_direct, P->d_evals, P->d_report, st));
   BTK_CUDA(cudaEventRecord(e[1], st));
   // Solve at the chosen degrees.
   Ptr4 o{}, w{}, wm{};
@@ -1458,7 +1550,8 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
                               S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
                               P->d_S4 + S.n_points, st));
-    BTK_CUDA(launch_resolve(P->dim, P->n_pc, P->d_pc_entry, P->d_pc_src_cluster, P->d_deg_pc, P->n_far, P->tiles_max,
+    BTK_CUDA(launch_resolve(P->dim, P->n_pc, P->d_pc_entry, P->d_pc_src_cluster, P->d_deg_pc, P->d_pc_direct,
+                            P->n_far, P->tiles_max,
                             P->d_far_type, P->d_far_tgt, P->d_far_src, P->d_deg_far, P->d_s_slot_off,
                             P->d_s_cluster_slot_begin, P->d_t_slot_off, P->d_t_cluster_slot_begin, P->degree_min,
                             T.n_points, S.n_points, P->d_tgt_centre, P->n_static_items, P->ictx.d_items,
@@ -1490,10 +1583,10 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   BTK_CUDA(launch_audit_compare(P->n_audit, P->ncomp, T.n_points, P->d_audit_orig, nullptr, out, P->d_audit_out,
                                 P->d_audit_sums, st));
   double sums[2] = {0, 0};
-  unsigned long long ev = 0;
+  unsigned long long ev[2] = {0, 0};  // far evaluations; direct ones of the leaf pairs kept direct
   int hist[kMaxNodes] = {0};  // degrees the selector chose (before any fallback)
   BTK_CUDA(cudaMemcpyAsync(sums, P->d_audit_sums, sizeof(sums), cudaMemcpyDeviceToHost, st));
-  BTK_CUDA(cudaMemcpyAsync(&ev, P->d_evals, sizeof(ev), cudaMemcpyDeviceToHost, st));
+  BTK_CUDA(cudaMemcpyAsync(ev, P->d_evals, sizeof(ev), cudaMemcpyDeviceToHost, st));
   BTK_CUDA(cudaMemcpyAsync(hist, P->d_report, sizeof(hist), cudaMemcpyDeviceToHost, st));
   BTK_CUDA(cudaStreamSynchronize(st));
   const double rel = std::sqrt(sums[0] / std::max(sums[1], 1e-300));
@@ -1505,9 +1598,11 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   }
   int fell_back = 0;
   if (!(rel <= tol)) {
-    // Fallback: the fixed-degree plain method (degree n everywhere, FP64).
+    // Fallback: the fixed-degree plain method (degree n everywhere, leaf pairs
+    // direct, FP64).
     fell_back = 1;
     BTK_CUDA(launch_fill_int(P->n_pairs, P->degree, P->d_deg_pc, st));
+    BTK_CUDA(launch_fill_int(P->n_pc - P->n_pc_list, 0, P->d_deg_pc + P->n_pc_list, st));
     InteractCtx plain = P->ictx;
     plain.precision = BTK_PREC_FP64;
     BTK_TRY(solve(plain));
@@ -1519,8 +1614,8 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     report->audit_rel_l2 = rel;
     report->audit_targets = P->n_audit;
     report->fell_back = fell_back;
-    report->evals_far = (int64_t)ev;
-    report->evals_near = P->evals[0];
+    report->evals_far = (int64_t)ev[0];
+    report->evals_near = P->evals[0] - P->conv_direct_total + (int64_t)ev[1];
     cudaEventElapsedTime(&report->ms_select, e[0], e[1]);
     cudaEventElapsedTime(&report->ms_solve, e[1], e[2]);
     cudaEventElapsedTime(&report->ms_total, e[0], e[3]);
@@ -1636,10 +1731,11 @@ btk_status btk_plan_set_degrees(btk_plan* P, const int* deg_pc, const int* deg_c
     return true;
   };
   const int n_cc = P->n_far - P->n_cp;
-  BTK_CHECK(!deg_pc || check(deg_pc, P->n_pc), BTK_ERR_INVALID_ARGUMENT, "PC degree outside [degree_min, degree]");
+  BTK_CHECK(!deg_pc || check(deg_pc, P->n_pc_list), BTK_ERR_INVALID_ARGUMENT,
+            "PC degree outside [degree_min, degree]");
   BTK_CHECK(!deg_cp || check(deg_cp, P->n_cp), BTK_ERR_INVALID_ARGUMENT, "CP degree outside [degree_min, degree]");
   BTK_CHECK(!deg_cc || check(deg_cc, n_cc), BTK_ERR_INVALID_ARGUMENT, "CC degree outside [degree_min, degree]");
-  if (deg_pc) std::copy(deg_pc, deg_pc + P->n_pc, P->h_deg_pc.begin());
+  if (deg_pc) std::copy(deg_pc, deg_pc + P->n_pc_list, P->h_deg_pc.begin());  // leaf pairs stay direct
   if (deg_cp) std::copy(deg_cp, deg_cp + P->n_cp, P->h_deg_far.begin());
   if (deg_cc) std::copy(deg_cc, deg_cc + n_cc, P->h_deg_far.begin() + P->n_cp);
   BTK_CUDA(cudaMemcpyAsync(P->d_deg_pc, P->h_deg_pc.data(), sizeof(int) * P->n_pc, cudaMemcpyHostToDevice, P->stream));

@@ -314,15 +314,25 @@ __global__ void k_adam(float* master, __nv_bfloat16* w, const float* grad, float
 }
 
 // Degree choice: the smallest d in [lo, hi] with prediction <= target, else hi.
-__global__ void k_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int* deg) {
+// Leaf pairs [conv0, n_pc) also have the direct evaluation (degree 0): taken
+// when no degree meets the target or when the source leaf has no more points
+// than the chosen degree's proxies (pc_direct[2 i + 1]).
+__global__ void k_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int dim, int conv0,
+                                 int n_pc, const int* pc_direct, int* deg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int d = hi;
+  bool met = false;
   for (int c = max(lo, kDegLo); c <= hi && c < kDegLo + kO; ++c)
     if (pred[(size_t)i * kO + (c - kDegLo)] <= log10_target) {
       d = c;
+      met = true;
       break;
     }
+  if (i >= conv0 && i < n_pc) {
+    const int m = d + 1, proxies = dim == 3 ? m * m * m : m * m;
+    if (!met || proxies >= pc_direct[2 * i + 1]) d = 0;
+  }
   deg[i] = d;
 }
 
@@ -334,14 +344,21 @@ __global__ void k_choose_degrees(int n, const float* pred, float log10_target, i
 // error. The Lagrangian of "fewest evaluations for a given sum of squared
 // errors over the targets": expensive pairs accept a larger error, cheap ones
 // a smaller one, where the uniform threshold gives every pair the same.
-__global__ void k_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, const float* pred, float log10_target,
-                                      int lo, int hi, const int* pc_tcount, const int* cp_scount, const int* weight,
-                                      float inv_cbar, float inv_wbar, int* deg) {
+// Leaf pairs [conv0, n_pc) also have the direct evaluation (degree 0): cost
+// target points x source points, no approximation error.
+__global__ void k_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, int conv0, const float* pred,
+                                      float log10_target, int lo, int hi, const int* pc_tcount, const int* cp_scount,
+                                      const int* pc_direct, const int* weight, float inv_cbar, float inv_wbar,
+                                      int* deg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float wr = (float)weight[i] * inv_wbar;
   float best = 3.4e38f;
   int d_best = hi;
+  if (i >= conv0 && i < n_pc) {
+    best = (float)pc_tcount[i] * (float)pc_direct[2 * i + 1] * inv_cbar;
+    d_best = 0;
+  }
   for (int c = max(lo, kDegLo); c <= hi && c < kDegLo + kO; ++c) {
     const float m = (float)(c + 1);
     const float md = dim == 3 ? m * m * m : m * m;
@@ -356,28 +373,36 @@ __global__ void k_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, const 
   deg[i] = d_best;
 }
 
-// Far-field evaluations at the chosen degrees (pairs PC, CP, CC in order).
+// Far-field evaluations at the chosen degrees (pairs PC, CP, CC in order) into
+// evals[0]; leaf pairs kept direct (degree 0) add their direct evaluations to
+// evals[1].
 __global__ void k_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
-                            const int* cp_scount, unsigned long long* evals, int* hist) {
+                            const int* cp_scount, const int* pc_direct, unsigned long long* evals, int* hist) {
   __shared__ int sh[kMaxDegree + 1];
   if (threadIdx.x <= kMaxDegree) sh[threadIdx.x] = 0;
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long v = 0;
+  unsigned long long v = 0, vd = 0;
   const int n = n_pc + n_cp + n_cc;
   if (i < n && deg[i] >= 0 && deg[i] <= kMaxDegree) atomicAdd(&sh[deg[i]], 1);
   if (i < n) {
     const unsigned long long m = (unsigned long long)(deg[i] + 1);
     const unsigned long long s = dim == 3 ? m * m * m : m * m;
-    if (i < n_pc)
+    if (i < n_pc && deg[i] == 0)
+      vd = (unsigned long long)pc_tcount[i] * (unsigned long long)pc_direct[2 * i + 1];
+    else if (i < n_pc)
       v = s * (unsigned long long)pc_tcount[i];
     else if (i < n_pc + n_cp)
       v = s * (unsigned long long)cp_scount[i - n_pc];
     else
       v = s * s;
   }
-  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  for (int off = 16; off > 0; off >>= 1) {
+    v += __shfl_down_sync(0xffffffffu, v, off);
+    vd += __shfl_down_sync(0xffffffffu, vd, off);
+  }
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(evals, v);
+  if ((threadIdx.x & 31) == 0 && vd) atomicAdd(evals + 1, vd);
   __syncthreads();
   if (threadIdx.x <= kMaxDegree && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
 }
@@ -595,10 +620,12 @@ __global__ void k_fill_int(int n, int value, int* dst) {
 int selector_param_count() { return kParams; }
 
 cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
-                             const int* cp_scount, unsigned long long* evals, int* hist, cudaStream_t s) {
+                             const int* cp_scount, const int* pc_direct, unsigned long long* evals, int* hist,
+                             cudaStream_t s) {
   const int n = n_pc + n_cp + n_cc;
   if (n <= 0) return cudaSuccess;
-  k_far_evals<<<(n + 255) / 256, 256, 0, s>>>(dim, n_pc, n_cp, n_cc, deg, pc_tcount, cp_scount, evals, hist);
+  k_far_evals<<<(n + 255) / 256, 256, 0, s>>>(dim, n_pc, n_cp, n_cc, deg, pc_tcount, cp_scount, pc_direct, evals,
+                                              hist);
   count_launch();
   return cudaGetLastError();
 }
@@ -678,20 +705,22 @@ cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const
   return cudaGetLastError();
 }
 
-cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int* deg,
-                                  cudaStream_t s) {
+cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int dim, int conv0,
+                                  int n_pc, const int* pc_direct, int* deg, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_choose_degrees<<<(n + 255) / 256, 256, 0, s>>>(n, pred, log10_target, lo, hi, deg);
+  k_choose_degrees<<<(n + 255) / 256, 256, 0, s>>>(n, pred, log10_target, lo, hi, dim, conv0, n_pc, pc_direct, deg);
   count_launch();
   return cudaGetLastError();
 }
 
-cudaError_t launch_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, const float* pred, float log10_target, int lo,
-                                       int hi, const int* pc_tcount, const int* cp_scount, const int* weight,
-                                       float inv_cbar, float inv_wbar, int* deg, cudaStream_t s) {
+cudaError_t launch_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, int conv0, const float* pred,
+                                       float log10_target, int lo, int hi, const int* pc_tcount, const int* cp_scount,
+                                       const int* pc_direct, const int* weight, float inv_cbar, float inv_wbar,
+                                       int* deg, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_choose_degrees_cost<<<(n + 255) / 256, 256, 0, s>>>(n, dim, n_pc, n_cp, pred, log10_target, lo, hi, pc_tcount,
-                                                        cp_scount, weight, inv_cbar, inv_wbar, deg);
+  k_choose_degrees_cost<<<(n + 255) / 256, 256, 0, s>>>(n, dim, n_pc, n_cp, conv0, pred, log10_target, lo, hi,
+                                                        pc_tcount, cp_scount, pc_direct, weight, inv_cbar, inv_wbar,
+                                                        deg);
   count_launch();
   return cudaGetLastError();
 }

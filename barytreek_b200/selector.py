@@ -104,6 +104,8 @@ def generate_samples(tc, charges, n_samples: int, K: int = 32, seed: int = 0, ba
     import torch
     L = load()
     rng = np.random.default_rng(seed)
+    if tc.stats()["leaf_far_pairs"]:
+        raise ValueError("error samples index the PC, CP and CC lists: use a plan without leaf_far_pairs")
     n_pairs = ctypes.c_int()
     check(L.btk_plan_pair_count(tc._plan, ctypes.byref(n_pairs)))
     n_pairs = n_pairs.value

@@ -229,14 +229,16 @@ class Treecode:
     with the bit-identical host functions (``device_tree=True``: the same tree
     and lists built on the GPU from the device copies of the points), then a device plan holds the
     leaf ordering, geometry and interaction work lists. ``cc_operators=True`` applies the CC pairs of
-    a fixed-degree plan as shared kernel matrices (pairs grouped by level and lattice offset). :meth:`solve` takes
+    a fixed-degree plan as shared kernel matrices (pairs grouped by level and lattice offset).
+    ``leaf_far_pairs=True`` (per-pair plans) lets the learned degree choice approximate well-separated
+    PP pairs as target points x source-leaf proxies, with the direct evaluation as an option. :meth:`solve` takes
     charges (numpy or a CUDA tensor) and returns a CUDA tensor
     ``[ncomp, n_targets]`` in the original point order.
     """
 
     def __init__(self, coords, sources=None, *, degree=8, cluster_size=100, theta=0.7, eps=1e-4, kind=KIND_POT,
                  precision=PREC_FP64, degree_mode=_lib.DEGREE_FIXED, degree_min=1, work_split=0, device_tree=False,
-                 cc_operators=False, device="cuda"):
+                 cc_operators=False, leaf_far_pairs=False, device="cuda"):
         import torch
 
         self.dim = len(coords)
@@ -244,6 +246,7 @@ class Treecode:
         self.degree_mode, self.degree_min = degree_mode, degree_min
         self.work_split = work_split
         self.cc_operators = bool(cc_operators)
+        self.leaf_far_pairs = bool(leaf_far_pairs)
         self.ncomp = ncomp(self.dim, kind)
         self.cfg = make_run_config(self.dim, degree, cluster_size, theta, eps)
         self.targets = tuple(np.ascontiguousarray(c, np.float64) for c in coords)
@@ -288,6 +291,7 @@ class Treecode:
         d.degree_mode, d.degree_min = self.degree_mode, self.degree_min
         d.work_split = self.work_split
         d.cc_operators = int(self.cc_operators)
+        d.leaf_far_pairs = int(self.leaf_far_pairs)
         stream = torch.cuda.current_stream(self.device).cuda_stream
         check(load().btk_plan_create(ctypes.byref(self._plan), ctypes.byref(d), stream))
 

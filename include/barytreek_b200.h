@@ -339,6 +339,18 @@ typedef struct {
    * ignored otherwise (btk_plan_stats.cc_groups = 0). 0: pairwise, as the
    * reference. */
   int cc_operators;
+  /* BTK_DEGREE_PER_PAIR plans only (no reference counterpart): 1 lets the
+   * degree choice approximate well-separated PP pairs too. The reference
+   * evaluates every pair of leaves directly once both have at most
+   * fmm_cluster_thresh points, a cost rule made for proxies at the plan
+   * degree; at a per-pair degree d, a pair of leaves that satisfies the MAC
+   * is cheaper as target points x source proxies when the source leaf has more
+   * than (d+1)^dim points. Such pairs join the PC pairs of the degree choice,
+   * with the direct evaluation as one more option (chosen when it is cheaper
+   * or when no degree meets the pair tolerance under the cost rule); the
+   * fallback and btk_plan_execute evaluate them directly, as the reference
+   * does. 0: PP pairs are always direct. */
+  int leaf_far_pairs;
 } btk_plan_desc;
 
 enum { BTK_DEGREE_FIXED = 0, BTK_DEGREE_PER_PAIR = 1 };
@@ -362,6 +374,7 @@ typedef struct {
   float build_ms_work;  /* of which the work-list builder (grouping, near/far split, items) */
   int cc_groups;        /* CC pair groups applied as shared matrices (0: pairwise CC) */
   int cc_tasks;         /* tasks of the CC-group launches (groups cut into pieces of <= 16 or 32 pairs) */
+  int leaf_far_pairs;   /* PP pairs the degree choice may approximate (btk_plan_desc.leaf_far_pairs) */
 } btk_plan_stats;
 btk_status btk_plan_stats_get(const btk_plan* plan, btk_plan_stats* stats);
 
@@ -425,12 +438,12 @@ typedef struct {
   double audit_rel_l2; /* treecode vs direct sum over the audited targets */
   int audit_targets;   /* 1% of the targets (fixed, seeded sample) */
   int fell_back;       /* 1: audit above tol, the fixed-degree FP64 result was returned */
-  int64_t evals_near;  /* PP evaluations */
+  int64_t evals_near;  /* PP evaluations (approximated leaf pairs excluded) */
   int64_t evals_far;   /* PC + CP + CC evaluations at the chosen degrees */
   float ms_select;     /* upward pass + features + network + degree choice */
   float ms_solve;      /* interactions + promotion + downward at the chosen degrees */
   float ms_total;      /* everything, audit and fallback included */
-  int degree_hist[13]; /* far-field pairs per chosen degree */
+  int degree_hist[13]; /* far-field pairs per chosen degree ([0]: leaf pairs kept direct) */
   float ms_kernel;     /* the interaction kernel of the learned solve (audit items included) */
   double pair_tol;     /* the per-pair tolerance this solve used */
 } btk_learned_report;

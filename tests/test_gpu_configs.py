@@ -10,9 +10,10 @@
   sphere, strengths U[-1,1], theta = 0.8: learned + mixed against plain FP64
   at n = 10.
 
-For the learned solves, after two settling solves the third must pass its
-audit without falling back, meet 1e-6 relative L2 against the FP64 direct sum
-at 2,000 sampled targets, and run faster than the plain solve.
+For the learned solves (well-separated leaf pairs approximable), after two
+settling solves the third must pass its audit without falling back, meet 1e-6
+relative L2 against the FP64 direct sum at 2,000 sampled targets, and run
+faster than the plain solve.
 """
 import os
 
@@ -72,7 +73,7 @@ def _learned_vs_plain(pts, q, kind, eps, theta, kind_name):
     idx, ds = _direct(plain, q, kind, eps)
     plain.close()
     lt = btk.Treecode(pts, degree=10, cluster_size=2000, theta=theta, eps=eps, kind=kind, precision=btk.PREC_MIXED,
-                      degree_mode=btk._lib.DEGREE_PER_PAIR, degree_min=4)
+                      degree_mode=btk._lib.DEGREE_PER_PAIR, degree_min=4, leaf_far_pairs=True)
     sel = selector.Selector.load(kind=kind)
     for _ in range(3):
         out, rep = lt.solve_learned(qd, sel, tol=1e-6)
@@ -127,7 +128,8 @@ def test_split_trees_at_scale():
     assert e_plain <= 2e-6
     mixed = btk.Treecode(tg, src, precision=btk.PREC_MIXED, **kw)
     assert rel(mixed.solve(qd).cpu().numpy()[:, idx], ds) <= e_plain + 1e-6
-    lt = btk.Treecode(tg, src, precision=btk.PREC_MIXED, degree_mode=_lib.DEGREE_PER_PAIR, degree_min=4, **kw)
+    lt = btk.Treecode(tg, src, precision=btk.PREC_MIXED, degree_mode=_lib.DEGREE_PER_PAIR, degree_min=4,
+                      leaf_far_pairs=True, **kw)
     sel = selector.Selector.load(kind=btk.KIND_FIELD)
     for _ in range(3):
         o, rep = lt.solve_learned(qd, sel, tol=2e-6)

@@ -1,0 +1,87 @@
+"""Well-separated leaf pairs in the learned degree choice (``leaf_far_pairs``).
+
+PP pairs that satisfy the traversal's MAC may be approximated as target
+points x source-leaf proxies at a chosen degree, or kept direct. With every
+degree in force at the plan degree (btk_plan_execute) they are direct, so the
+plan must reproduce the plan without them; learned solves must keep the
+1e-6 accuracy against the FP64 direct sum, pass their audit without falling
+back, and evaluate fewer pairs directly.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def _direct(tc, q, kind, eps, m=2000, seed=99):
+    import torch
+    from barytreek_b200 import _lib
+    L = _lib.load()
+    idx = np.sort(np.random.default_rng(seed).choice(tc.nt, m, replace=False))
+    t = [torch.from_numpy(np.ascontiguousarray(c[idx])).cuda() for c in tc.targets]
+    out = torch.empty((tc.ncomp, m), dtype=torch.float64, device="cuda")
+    qd = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    s = tc._s
+    z = lambda a: _lib.ptr(a[2]) if tc.dim == 3 else None
+    _lib.check(L.btk_direct_sum(tc.dim, kind, eps, m, _lib.ptr(t[0]), _lib.ptr(t[1]), z(t), tc.nt, _lib.ptr(s[0]),
+                                _lib.ptr(s[1]), z(s), _lib.ptr(qd), _lib.ptr(out), None))
+    return idx, out.cpu().numpy()
+
+
+def test_degrees_in_force_keep_leaf_pairs_direct():
+    import barytreek_b200 as btk
+    from barytreek_b200 import _lib, datagen
+    pts, q = datagen.uniform_box(3, 200_000, 3, 0.0, 1.0)
+    kw = dict(degree=6, cluster_size=500, theta=0.7, eps=1e-4, kind=btk.KIND_FIELD, precision=btk.PREC_MIXED,
+              degree_mode=_lib.DEGREE_PER_PAIR, degree_min=4)
+    a = btk.Treecode(pts, **kw)
+    b = btk.Treecode(pts, leaf_far_pairs=True, **kw)
+    sb = b.stats()
+    assert a.stats()["leaf_far_pairs"] == 0 and sb["leaf_far_pairs"] > 0
+    assert sb["evals_pp"] == a.stats()["evals_pp"] and b.evals() == a.evals()
+    ra, rb = a.solve(q).cpu().numpy(), b.solve(q).cpu().numpy()
+    assert rel(rb, ra) <= 1e-14
+    # per-list degrees leave the leaf pairs direct
+    pc = len(b.lists[1])
+    b.set_degrees(deg_pc=np.full(pc, 4, np.int32))
+    a.set_degrees(deg_pc=np.full(pc, 4, np.int32))
+    assert rel(b.solve(q).cpu().numpy(), a.solve(q).cpu().numpy()) <= 1e-14
+
+
+@pytest.mark.parametrize("case", ["uniform-field-1m", "plummer-pot-1m", "mixture-field-262k"])
+def test_learned_with_leaf_pairs(case):
+    import torch
+
+    import barytreek_b200 as btk
+    from barytreek_b200 import _lib, datagen, selector
+    if case == "uniform-field-1m":
+        pts, q = datagen.uniform_box(1, 1 << 20, 3, 0.0, 1.0)
+        kind, leaf, deg = btk.KIND_FIELD, 2000, 8
+    elif case == "plummer-pot-1m":
+        pts, q = datagen.plummer(2, 1 << 20)
+        kind, leaf, deg = btk.KIND_POT, 2000, 8
+    else:
+        pts, q = datagen.gaussian_mixture(3, 1 << 18)
+        kind, leaf, deg = btk.KIND_FIELD, 1000, 8
+    qd = torch.from_numpy(q).cuda()
+    kw = dict(degree=deg, cluster_size=leaf, theta=0.7, eps=1e-4, kind=kind, precision=btk.PREC_MIXED,
+              degree_mode=_lib.DEGREE_PER_PAIR, degree_min=4)
+    sel = selector.Selector.load(kind=kind)
+    base = btk.Treecode(pts, **kw)
+    for _ in range(3):
+        _, rb = base.solve_learned(qd, sel, tol=1e-6)
+    base.close()
+    tc = btk.Treecode(pts, leaf_far_pairs=True, **kw)
+    for _ in range(3):
+        out, rep = tc.solve_learned(qd, sel, tol=1e-6)
+    idx, ds = _direct(tc, q, kind, 1e-4)
+    err = rel(out.cpu().numpy()[:, idx], ds)
+    assert rep["fell_back"] == 0, rep
+    assert rep["audit_rel_l2"] <= 1e-6
+    assert err <= 1e-6, err
+    assert rep["evals_near"] < rb["evals_near"]
+    assert rep["ms_total"] < rb["ms_total"], (rep["ms_total"], rb["ms_total"])
