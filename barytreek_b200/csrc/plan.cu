@@ -676,7 +676,7 @@ struct btk_plan {
   std::vector<int> h_pc_tcount, h_cp_scount, h_deg_pc, h_deg_far;
 
   // ---- learned selector (per-pair plans) ----
-  int n_pairs = 0;  // PC, then CP, then CC
+  int n_pairs = 0;  // PC (the list, then the leaf pairs), then CP, then CC
   int *d_pair_type = nullptr, *d_pair_tgt = nullptr, *d_pair_src = nullptr;
   int *d_pc_tcount = nullptr, *d_cp_scount = nullptr;
   float *d_desc = nullptr, *d_feat = nullptr, *d_pred = nullptr;
@@ -971,7 +971,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   {
     std::vector<int> all(std::max(P->n_pairs, 1), n);
     std::fill(all.begin() + P->n_pc_list, all.begin() + P->n_pc, 0);
-    BTK_TRY(A.upload(&P->d_deg_pc, all));  // one array: PC degrees, then CP, then CC
+    BTK_TRY(A.upload(&P->d_deg_pc, all));  // one array: PC (list, leaf pairs) degrees, then CP, then CC
     P->d_deg_far = P->d_deg_pc + P->n_pc;
   }
   recount_far_evals(P);

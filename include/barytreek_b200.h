@@ -427,7 +427,8 @@ btk_status btk_selector_create(btk_selector** sel, const float* params, const fl
 btk_status btk_selector_destroy(btk_selector* sel);
 const void* btk_selector_weights(const btk_selector* sel); /* device BF16 parameters */
 
-/* Far-field pairs of a per-pair plan (PC, then CP, then CC, list order). */
+/* Far-field pairs of a per-pair plan (PC, then CP, then CC, list order; with
+ * leaf_far_pairs the leaf pairs follow the PC list). */
 btk_status btk_plan_pair_count(const btk_plan* plan, int* n_pairs);
 /* Runs the upward pass for these sources/charges and writes the features of
  * every far-field pair: device float features[n_pairs][16]. */
