@@ -148,6 +148,7 @@ SIGNATURES = {
     "btk_selector_destroy": [_vp],
     "btk_selector_weights": [_vp],
     "btk_plan_pair_count": [_vp, _vp],
+    "btk_selector_predict": [_vp, _ci, _vp, _vp, _vp],
     "btk_plan_pair_features": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_plan_execute_learned": [_vp, _vp, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_plan_error_samples": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _ci, _vp, _ci, _vp, _vp, _vp, _vp, _vp, _vp],

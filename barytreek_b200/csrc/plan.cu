@@ -1476,6 +1476,14 @@ btk_status btk_selector_destroy(btk_selector* s) {
 
 const void* btk_selector_weights(const btk_selector* s) { return s ? s->d_w : nullptr; }
 
+btk_status btk_selector_predict(const btk_selector* s, int n, const float* features, float* out,
+                                btk_stream_t stream) {
+  BTK_CHECK(s && n >= 0 && (n == 0 || (features && out)), BTK_ERR_INVALID_ARGUMENT,
+            "btk_selector_predict: bad argument");
+  BTK_CUDA(launch_mlp_infer(n, s->d_w, s->norm, features, out, (cudaStream_t)stream));
+  return BTK_OK;
+}
+
 btk_status btk_plan_pair_count(const btk_plan* P, int* n_pairs) {
   BTK_CHECK(P && n_pairs, BTK_ERR_INVALID_ARGUMENT, "null argument");
   BTK_CHECK(P->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT, "plan is not BTK_DEGREE_PER_PAIR");

@@ -205,18 +205,136 @@ __device__ __forceinline__ void mlp_row(const float* sw, const float* x, float* 
     for (int j = 0; j < kH; ++j) h2o[j] = h2[j];
 }
 
-// Inference on raw features: out[i][o] = predicted log10 error at degree 4+o.
+// Inference on raw features, out[i][o] = predicted log10 error at degree 4+o,
+// on the tensor cores: each warp pushes 16 pairs through the three layers as
+// mma.sync m16n8k16 BF16 products with FP32 accumulation (layer 1: 8 column
+// tiles of K = 16; layer 2: 8 x 4 of K = 64; layer 3: 2 column tiles, outputs
+// 9..15 zero). The accumulator layout of one layer (rows g and g + 8, columns
+// 2t, 2t + 1 of each 8-column tile, g = lane / 4, t = lane % 4) is the A
+// operand layout of the next layer's K = 16 steps, so activations stay in
+// registers: bias, ReLU and the round to BF16 are applied in place. Weights
+// sit in shared memory as BF16 rows padded to 24 / 72 elements, which puts the
+// 32 lanes' B-operand words in 32 different banks. Normalised inputs and
+// hidden activations are rounded to BF16 (the training kernels keep them in
+// FP32; the difference is within the network's error).
+constexpr int kW1Row = kF + 8, kW2Row = kH + 8;  // padded BF16 row lengths
+struct InferSmem {
+  __nv_bfloat16 w1[kH * kW1Row], w2[kH * kW2Row], w3[16 * kW2Row];
+  float b1[kH], b2[kH], b3[16];
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
 __global__ void __launch_bounds__(128) k_mlp_infer(int n, const __nv_bfloat16* w, MlpNorm nrm, const float* feat,
                                                    float* out) {
-  extern __shared__ float sw[];
-  load_params(w, sw);
+  __shared__ __align__(16) InferSmem sm;
+  for (int o = threadIdx.x; o < kH * kW1Row; o += blockDim.x) {
+    const int r = o / kW1Row, c = o % kW1Row;
+    sm.w1[o] = c < kF ? w[kW1 + r * kF + c] : __float2bfloat16(0.f);
+  }
+  for (int o = threadIdx.x; o < kH * kW2Row; o += blockDim.x) {
+    const int r = o / kW2Row, c = o % kW2Row;
+    sm.w2[o] = c < kH ? w[kW2 + r * kH + c] : __float2bfloat16(0.f);
+  }
+  for (int o = threadIdx.x; o < 16 * kW2Row; o += blockDim.x) {
+    const int r = o / kW2Row, c = o % kW2Row;
+    sm.w3[o] = (r < kO && c < kH) ? w[kW3 + r * kH + c] : __float2bfloat16(0.f);
+  }
+  for (int o = threadIdx.x; o < kH; o += blockDim.x) {
+    sm.b1[o] = __bfloat162float(w[kB1 + o]);
+    sm.b2[o] = __bfloat162float(w[kB2 + o]);
+  }
+  if (threadIdx.x < 16) sm.b3[threadIdx.x] = threadIdx.x < kO ? __bfloat162float(w[kB3 + threadIdx.x]) : 0.f;
   __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float x[kF], y[kO];
-  for (int k = 0; k < kF; ++k) x[k] = (feat[(size_t)i * kF + k] - nrm.xm[k]) / nrm.xs[k];
-  mlp_row(sw, x, y, nullptr, nullptr);
-  for (int o = 0; o < kO; ++o) out[(size_t)i * kO + o] = y[o] * nrm.ys + nrm.ym;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int tile = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 16 < n; tile += warps) {
+    const int r0 = tile * 16 + g, r1 = r0 + 8;  // this lane's two pairs
+    // layer 1 A operand: normalised features, columns 2t, 2t + 1 and 2t + 8, 2t + 9
+    float x[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = h ? r1 : r0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int c = 2 * t + (q & 1) + (q >> 1) * 8;
+        x[h][q] = r < n ? (feat[(size_t)r * kF + c] - nrm.xm[c]) / nrm.xs[c] : 0.f;
+      }
+    }
+    const uint32_t a10 = pack_bf16x2(x[0][0], x[0][1]), a11 = pack_bf16x2(x[1][0], x[1][1]);
+    const uint32_t a12 = pack_bf16x2(x[0][2], x[0][3]), a13 = pack_bf16x2(x[1][2], x[1][3]);
+    float h1[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const __nv_bfloat16* wr = sm.w1 + (8 * j + g) * kW1Row + 2 * t;
+      h1[j][0] = h1[j][1] = h1[j][2] = h1[j][3] = 0.f;
+      mma_bf16(h1[j], a10, a11, a12, a13, *reinterpret_cast<const uint32_t*>(wr),
+               *reinterpret_cast<const uint32_t*>(wr + 8));
+      const int c = 8 * j + 2 * t;
+      h1[j][0] = fmaxf(h1[j][0] + sm.b1[c], 0.f);
+      h1[j][1] = fmaxf(h1[j][1] + sm.b1[c + 1], 0.f);
+      h1[j][2] = fmaxf(h1[j][2] + sm.b1[c], 0.f);
+      h1[j][3] = fmaxf(h1[j][3] + sm.b1[c + 1], 0.f);
+    }
+    uint32_t a2[4][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      a2[kk][0] = pack_bf16x2(h1[2 * kk][0], h1[2 * kk][1]);
+      a2[kk][1] = pack_bf16x2(h1[2 * kk][2], h1[2 * kk][3]);
+      a2[kk][2] = pack_bf16x2(h1[2 * kk + 1][0], h1[2 * kk + 1][1]);
+      a2[kk][3] = pack_bf16x2(h1[2 * kk + 1][2], h1[2 * kk + 1][3]);
+    }
+    float h2[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      h2[j][0] = h2[j][1] = h2[j][2] = h2[j][3] = 0.f;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const __nv_bfloat16* wr = sm.w2 + (8 * j + g) * kW2Row + 16 * kk + 2 * t;
+        mma_bf16(h2[j], a2[kk][0], a2[kk][1], a2[kk][2], a2[kk][3], *reinterpret_cast<const uint32_t*>(wr),
+                 *reinterpret_cast<const uint32_t*>(wr + 8));
+      }
+      const int c = 8 * j + 2 * t;
+      h2[j][0] = fmaxf(h2[j][0] + sm.b2[c], 0.f);
+      h2[j][1] = fmaxf(h2[j][1] + sm.b2[c + 1], 0.f);
+      h2[j][2] = fmaxf(h2[j][2] + sm.b2[c], 0.f);
+      h2[j][3] = fmaxf(h2[j][3] + sm.b2[c + 1], 0.f);
+    }
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      a2[kk][0] = pack_bf16x2(h2[2 * kk][0], h2[2 * kk][1]);
+      a2[kk][1] = pack_bf16x2(h2[2 * kk][2], h2[2 * kk][3]);
+      a2[kk][2] = pack_bf16x2(h2[2 * kk + 1][0], h2[2 * kk + 1][1]);
+      a2[kk][3] = pack_bf16x2(h2[2 * kk + 1][2], h2[2 * kk + 1][3]);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      float y[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const __nv_bfloat16* wr = sm.w3 + (8 * j + g) * kW2Row + 16 * kk + 2 * t;
+        mma_bf16(y, a2[kk][0], a2[kk][1], a2[kk][2], a2[kk][3], *reinterpret_cast<const uint32_t*>(wr),
+                 *reinterpret_cast<const uint32_t*>(wr + 8));
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int c = 8 * j + 2 * t + (q & 1), r = (q >> 1) ? r1 : r0;
+        if (c < kO && r < n) out[(size_t)r * kO + c] = (y[q] + sm.b3[c]) * nrm.ys + nrm.ym;
+      }
+    }
+  }
 }
 
 // Forward on normalised inputs (training/validation): yn[i][o].
@@ -698,9 +816,14 @@ cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const
   }
   nrm.ym = norm[2 * kF];
   nrm.ys = norm[2 * kF + 1] > 0 ? norm[2 * kF + 1] : 1.f;
-  const size_t shm = sizeof(float) * kParams;
-  cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  k_mlp_infer<<<(n + 127) / 128, 128, shm, s>>>(n, (const __nv_bfloat16*)w_bf16, nrm, feat, out);
+  // 16 pairs per warp, 4 warps per block; at most 8 blocks per SM's worth of
+  // blocks, each looping over its tiles (the weights are staged once per block)
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int tiles = (n + 15) / 16;
+  const int grid = std::max(1, std::min((tiles + 3) / 4, 8 * sms));
+  k_mlp_infer<<<grid, 128, 0, s>>>(n, (const __nv_bfloat16*)w_bf16, nrm, feat, out);
   count_launch();
   return cudaGetLastError();
 }

@@ -426,6 +426,12 @@ int btk_selector_param_count(void);
 btk_status btk_selector_create(btk_selector** sel, const float* params, const float* norm);
 btk_status btk_selector_destroy(btk_selector* sel);
 const void* btk_selector_weights(const btk_selector* sel); /* device BF16 parameters */
+/* The network on raw features: out[i][o] = predicted log10 error at degree
+ * 4 + o (device arrays features[n][16], out[n][9]). Runs on the tensor cores
+ * (BF16 operands, FP32 accumulation; normalised inputs and hidden activations
+ * rounded to BF16). */
+btk_status btk_selector_predict(const btk_selector* sel, int n, const float* features, float* out,
+                                btk_stream_t stream);
 
 /* Far-field pairs of a per-pair plan (PC, then CP, then CC, list order; with
  * leaf_far_pairs the leaf pairs follow the PC list). */

@@ -42,6 +42,17 @@ def forward(p, x):
     return y, (x, z1, h1, z2, h2)
 
 
+def forward_bf16_activations(p, x):
+    """forward() with the inputs and both hidden activations rounded to BF16
+    (round to nearest even) before each layer, as the tensor-core inference
+    kernel feeds its BF16 operands; products and sums in FP64."""
+    w = unpack(p)
+    xb = bf16_round(x)
+    h1 = bf16_round(np.maximum(xb @ w["W1"].T + w["b1"], 0))
+    h2 = bf16_round(np.maximum(h1 @ w["W2"].T + w["b2"], 0))
+    return h2 @ w["W3"].T + w["b3"]
+
+
 def loss_and_grad(p, x, t, mask):
     n = len(x)
     y, (x, z1, h1, z2, h2) = forward(p, x)

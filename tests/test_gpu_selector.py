@@ -2,6 +2,7 @@
 
 * BF16 MLP kernels (forward, gradient, Adam) against the FP64 numpy oracle on
   the same BF16-rounded weights; tolerance relative L2 <= 1e-4 (FP32 sums).
+  The tensor-core inference against the oracle with BF16 activations (2e-3).
 * Training samples (per-degree pair errors) against the CPU oracle evaluating
   the same single pair at the same degree and the direct sum; the log10 errors
   agree to 0.05 where the error is above 1e-11.
@@ -54,6 +55,44 @@ def test_mlp_forward_and_gradient_match_oracle(batch, lib):
     l_ref, g_ref = mlp.loss_and_grad(pb, x.astype(np.float64), t.astype(np.float64), m.astype(np.float64))
     assert abs(loss.item() - l_ref) <= 1e-4 * abs(l_ref)
     assert rel(grad.cpu().numpy(), g_ref) <= 1e-4
+
+
+def test_tensor_core_inference_matches_oracle(batch, lib):
+    """btk_selector_predict (mma.sync BF16 products, FP32 sums, BF16-rounded
+    inputs and activations) against the FP64 oracle of the same rounding:
+    relative L2 <= 2e-3 (FP32 accumulation order and the rare activation whose
+    BF16 rounding flips); against the FP32-activation forward kernel <= 2e-2.
+    1,003 pairs: a partial 16-pair tile at the end, and a normalisation that
+    shifts and scales every input and output."""
+    import ctypes
+
+    import torch
+    from barytreek_b200 import _lib
+    from oracle import mlp
+    p, _, _, _ = batch
+    rng = np.random.default_rng(7)
+    n = 1003
+    xm = rng.standard_normal(mlp.F).astype(np.float32)
+    xs = (0.5 + rng.random(mlp.F)).astype(np.float32)
+    norm = np.concatenate([xm, xs, [0.7, 1.9]]).astype(np.float32)
+    feat = (xm + xs * rng.standard_normal((n, mlp.F))).astype(np.float32)
+    sel = ctypes.c_void_p()
+    _lib.check(lib.btk_selector_create(ctypes.byref(sel), _lib.ptr(p), _lib.ptr(norm)))
+    try:
+        F = torch.from_numpy(feat).cuda()
+        out = torch.full((n, mlp.O), float("nan"), dtype=torch.float32, device="cuda")
+        _lib.check(lib.btk_selector_predict(sel, n, _lib.ptr(F), _lib.ptr(out), None))
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+    finally:
+        lib.btk_selector_destroy(sel)
+    xn = (feat - xm) / xs
+    pb = mlp.bf16_round(p)
+    ref = mlp.forward_bf16_activations(pb, xn.astype(np.float32)) * 1.9 + 0.7
+    assert np.isfinite(got).all()
+    assert rel(got, ref) <= 2e-3
+    ref32, _ = mlp.forward(pb, xn.astype(np.float64))
+    assert rel(got, ref32 * 1.9 + 0.7) <= 2e-2
 
 
 def test_adam_step_matches_oracle(batch, lib):
