@@ -418,14 +418,12 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
       const int cnt = min(kChunk, w.s_total - c * kChunk);
       const int near_end = min(cnt, max(0, w.near_total - c * kChunk));  // near sources of this chunk
       const int b = c & 1;
-      // Potential and potential + gradient: a chunk with near-field sources
-      // is laid out per warp region (the 64 sources warp r converts fill pairs
-      // [32 r, 32 r + 32)): the near sources closer to the target box than
-      // max(hx, hy, hz) first, on the hi/lo path; the others after them, on
-      // the FP32 path (their separation is at least as large as a
-      // non-touching leaf's). The vector kernel keeps every near source on the
-      // hi/lo path.
-      const bool split = KIND != BTK_KIND_VEL && near_end > 0;  // block-uniform
+      // A chunk with near-field sources is laid out per warp region (the 64
+      // sources warp r converts fill pairs [32 r, 32 r + 32)): the near
+      // sources closer to the target box than max(hx, hy, hz) first, on the
+      // hi/lo path; the others after them, on the FP32 path (their separation
+      // is at least as large as a non-touching leaf's).
+      const bool split = near_end > 0;  // block-uniform
       {  // thread tid converts source pair tid into buffer b
         float hx[2], hy[2], hz[2], lx[2], ly[2], lz[2], ww[2];
         bool close[2];
@@ -437,13 +435,9 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
             split_rel(s.x, w.cx, hx[k], lx[k]);
             split_rel(s.y, w.cy, hy[k], ly[k]);
             split_rel(s.z, w.cz, hz[k], lz[k]);
-            if constexpr (KIND != BTK_KIND_VEL) {
-              const float gap = fmaxf(fabsf(hx[k]) - w.hx,
-                                      fmaxf(fabsf(hy[k]) - w.hy, DIM == 3 ? fabsf(hz[k]) - w.hz : -3.0e38f));
-              close[k] = j < near_end && gap < thr;
-            } else {
-              close[k] = false;
-            }
+            const float gap = fmaxf(fabsf(hx[k]) - w.hx,
+                                    fmaxf(fabsf(hy[k]) - w.hy, DIM == 3 ? fabsf(hz[k]) - w.hz : -3.0e38f));
+            close[k] = j < near_end && gap < thr;
             hx[k] = -hx[k];
             hy[k] = -hy[k];
             hz[k] = -hz[k];
