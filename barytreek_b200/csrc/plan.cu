@@ -655,7 +655,7 @@ struct btk_plan {
   // Leaf pairs the degree choice may approximate (leaf_far_pairs): PC-block
   // pairs [n_pc_list, n_pc), degree 0 = direct.
   int leaf_far = 0, n_pc_list = 0;
-  double theta = 0.7;
+  double leaf_theta = 0.8;  // separation bound of the leaf pairs
   int64_t conv_direct_total = 0;  // their direct evaluations (all included in evals[0])
   int* d_pc_direct = nullptr;
   int n_src_slots = 0, n_tgt_slots = 0;
@@ -785,7 +785,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     return o;
   };
   // Leaf pairs the degree choice may approximate: PP pairs that satisfy the
-  // MAC of the traversal, (r_t + r_s) / |c_t - c_s| < theta with r the
+  // traversal's MAC form, (r_t + r_s) / |c_t - c_s| < leaf_theta with r the
   // panels' half diagonals (src/interaction_list.cpp:142-156), whose source
   // leaf has more points than the proxies of degree_min. Their source leaves
   // get degree slots after the clusters'.
@@ -815,7 +815,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
         side = std::min(side, a.hi[d] - a.lo[d]);
       }
       const double dist = std::sqrt(d2);
-      if (dist > 0 && gap > 0.5 * side && (0.5 * std::sqrt(ra) + 0.5 * std::sqrt(rb)) / dist < P->theta)
+      if (dist > 0 && gap > 0.5 * side && (0.5 * std::sqrt(ra) + 0.5 * std::sqrt(rb)) / dist < P->leaf_theta)
         conv.push_back(i);
     }
     for (int i : conv) {
@@ -1115,7 +1115,8 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
   BTK_TRY(A.alloc(&P->d_ptw, (size_t)P->ncomp * Pt * P->ipc));
   P->degree_mode = D->degree_mode;
   P->leaf_far = D->degree_mode == BTK_DEGREE_PER_PAIR && D->leaf_far_pairs ? 1 : 0;
-  P->theta = cfg.fmm_theta;
+  BTK_CHECK(std::isfinite(D->leaf_far_theta), BTK_ERR_INVALID_ARGUMENT, "leaf_far_theta must be finite");
+  P->leaf_theta = D->leaf_far_theta > 0 ? D->leaf_far_theta : std::max(cfg.fmm_theta, 0.8);
   P->degree_min = D->degree_min;
   BTK_CHECK(D->work_split >= 0 && D->work_split <= 1024, BTK_ERR_INVALID_ARGUMENT, "work_split outside 0..1024");
   P->work_split = D->work_split > 0 ? D->work_split : 8;

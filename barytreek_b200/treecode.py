@@ -238,7 +238,7 @@ class Treecode:
 
     def __init__(self, coords, sources=None, *, degree=8, cluster_size=100, theta=0.7, eps=1e-4, kind=KIND_POT,
                  precision=PREC_FP64, degree_mode=_lib.DEGREE_FIXED, degree_min=1, work_split=0, device_tree=False,
-                 cc_operators=False, leaf_far_pairs=False, device="cuda"):
+                 cc_operators=False, leaf_far_pairs=False, leaf_far_theta=0.0, device="cuda"):
         import torch
 
         self.dim = len(coords)
@@ -247,6 +247,7 @@ class Treecode:
         self.work_split = work_split
         self.cc_operators = bool(cc_operators)
         self.leaf_far_pairs = bool(leaf_far_pairs)
+        self.leaf_far_theta = float(leaf_far_theta)
         self.ncomp = ncomp(self.dim, kind)
         self.cfg = make_run_config(self.dim, degree, cluster_size, theta, eps)
         self.targets = tuple(np.ascontiguousarray(c, np.float64) for c in coords)
@@ -292,6 +293,7 @@ class Treecode:
         d.work_split = self.work_split
         d.cc_operators = int(self.cc_operators)
         d.leaf_far_pairs = int(self.leaf_far_pairs)
+        d.leaf_far_theta = self.leaf_far_theta
         stream = torch.cuda.current_stream(self.device).cuda_stream
         check(load().btk_plan_create(ctypes.byref(self._plan), ctypes.byref(d), stream))
 

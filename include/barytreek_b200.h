@@ -351,6 +351,11 @@ typedef struct {
    * fallback and btk_plan_execute evaluate them directly, as the reference
    * does. 0: PP pairs are always direct. */
   int leaf_far_pairs;
+  /* The separation bound of those pairs: non-touching leaf pairs with
+   * (r_t + r_s) / |c_t - c_s| < leaf_far_theta (r: half diagonals) join the
+   * choice. <= 0: max(fmm_theta, 0.8), the largest MAC parameter the shipped
+   * selector was trained on. */
+  double leaf_far_theta;
 } btk_plan_desc;
 
 enum { BTK_DEGREE_FIXED = 0, BTK_DEGREE_PER_PAIR = 1 };

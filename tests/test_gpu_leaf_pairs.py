@@ -1,6 +1,7 @@
 """Well-separated leaf pairs in the learned degree choice (``leaf_far_pairs``).
 
-PP pairs that satisfy the traversal's MAC may be approximated as target
+Non-touching PP pairs within the separation bound (``leaf_far_theta``, default
+0.8) may be approximated as target
 points x source-leaf proxies at a chosen degree, or kept direct. With every
 degree in force at the plan degree (btk_plan_execute) they are direct, so the
 plan must reproduce the plan without them; learned solves must keep the
@@ -45,6 +46,11 @@ def test_degrees_in_force_keep_leaf_pairs_direct():
     assert sb["evals_pp"] == a.stats()["evals_pp"] and b.evals() == a.evals()
     ra, rb = a.solve(q).cpu().numpy(), b.solve(q).cpu().numpy()
     assert rel(rb, ra) <= 1e-14
+    # the separation bound: the traversal's theta admits fewer pairs than the default 0.8
+    c = btk.Treecode(pts, leaf_far_pairs=True, leaf_far_theta=0.7, **kw)
+    assert 0 < c.stats()["leaf_far_pairs"] < sb["leaf_far_pairs"]
+    assert rel(c.solve(q).cpu().numpy(), ra) <= 1e-14
+    c.close()
     # per-list degrees leave the leaf pairs direct
     pc = len(b.lists[1])
     b.set_degrees(deg_pc=np.full(pc, 4, np.int32))
