@@ -200,7 +200,7 @@ cudaError_t launch_fill_int(int n, int value, int* dst, cudaStream_t s);
 cudaError_t launch_src_slots(int dim, int n, int n_slots, const int* slot_cluster_panel, const int* slot_degree,
                              const long long* slot_offset, const DevPanel* panels, const double* psw,
                              const double* amat, const int* amat_off, const double* ucos_all, const int* ucos_off,
-                             double4* S4, cudaStream_t s);
+                             const int* used, double4* S4, cudaStream_t s);  // used: per slot, 0 = skip (NULL: all)
 cudaError_t launch_tgt_slots(int dim, int n_slots, const int* slot_cluster_panel, const int* slot_degree,
                              const long long* slot_offset, const DevPanel* panels, const double* ucos_all,
                              const int* ucos_off, double4* T4, int* T_out, long long t4_base, cudaStream_t s);
@@ -213,6 +213,6 @@ cudaError_t launch_resolve(int dim, int n_pc, const int* pc_entry, const int* pc
                            const int* cluster_slot_begin_s, const long long* tgt_slot_offset,
                            const int* cluster_slot_begin_t, int slot_d_lo, long long t4_base, long long s4_base,
                            const double* tgt_centre, int n_point_items, WorkItem* items, Entry* entries,
-                           int far_item0, int far_entry0, cudaStream_t s);
+                           int far_item0, int far_entry0, int* slot_used, cudaStream_t s);  // marks the source slots read
 
 }  // namespace btk

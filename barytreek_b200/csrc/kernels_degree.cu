@@ -56,9 +56,10 @@ __global__ void __launch_bounds__(256) k_src_slots(int dim, int n, const int* sl
                                                    const int* slot_degree, const long long* slot_offset,
                                                    const DevPanel* panels, const double* psw, const double* amat,
                                                    const int* amat_off, const double* ucos_all, const int* ucos_off,
-                                                   double4* S4) {
+                                                   const int* used, double4* S4) {
   __shared__ double bufA[kMaxIpc], bufB[kMaxIpc];
   const int slot = blockIdx.x;
+  if (used && !used[slot]) return;  // no pair reads this slot this solve
   const int P = slot_cluster_panel[slot], d = slot_degree[slot];
   const int mn = n + 1, md = d + 1;
   const int ipc_n = dim == 3 ? mn * mn * mn : mn * mn;
@@ -203,7 +204,7 @@ __device__ __forceinline__ int ipow_d(int b, int dim) { return dim == 3 ? b * b 
 // leaf's points, pc_direct[2 i] (first) and [2 i + 1] (count).
 __global__ void k_resolve_pc(int dim, int n_pc, const int* pc_entry, const int* pc_src_cluster, const int* degree,
                              const int* pc_direct, const long long* src_slot_offset, const int* cluster_slot_begin_s,
-                             int slot_d_lo, long long s4_base, Entry* entries) {
+                             int slot_d_lo, long long s4_base, Entry* entries, int* slot_used) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_pc) return;
   const int d = degree[i];
@@ -215,6 +216,7 @@ __global__ void k_resolve_pc(int dim, int n_pc, const int* pc_entry, const int* 
     const int slot = cluster_slot_begin_s[pc_src_cluster[i]] + (d - slot_d_lo);
     e.s_begin = (int)(s4_base + src_slot_offset[slot]);
     e.s_count = ipow_d(d + 1, dim);
+    if (slot_used) slot_used[slot] = 1;
   }
   const int k = pc_entry[i];
   if (k >= 0) entries[k] = e;
@@ -237,7 +239,7 @@ __global__ void k_far_items(int dim, int n_far, int tiles_max, const int* far_ty
                             const int* cluster_slot_begin_t, const long long* src_slot_offset,
                             const int* cluster_slot_begin_s, int slot_d_lo, long long t4_base, long long s4_base,
                             const double* tgt_centre, WorkItem* items, Entry* entries, int far_item0,
-                            int far_entry0) {
+                            int far_entry0, int* slot_used) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_far) return;
   const int d = degree[i];
@@ -250,6 +252,7 @@ __global__ void k_far_items(int dim, int n_far, int tiles_max, const int* far_ty
     const int slot = cluster_slot_begin_s[far_src[2 * i]] + (d - slot_d_lo);
     e.s_begin = (int)(s4_base + src_slot_offset[slot]);
     e.s_count = ipc_d;
+    if (slot_used) slot_used[slot] = 1;
   }
   entries[far_entry0 + i] = e;
   const int tc = far_tgt_cluster[i];
@@ -277,10 +280,10 @@ __global__ void k_far_items(int dim, int n_far, int tiles_max, const int* far_ty
 cudaError_t launch_src_slots(int dim, int n, int n_slots, const int* slot_cluster_panel, const int* slot_degree,
                              const long long* slot_offset, const DevPanel* panels, const double* psw,
                              const double* amat, const int* amat_off, const double* ucos_all, const int* ucos_off,
-                             double4* S4, cudaStream_t s) {
+                             const int* used, double4* S4, cudaStream_t s) {
   if (n_slots <= 0) return cudaSuccess;
   k_src_slots<<<n_slots, 256, 0, s>>>(dim, n, slot_cluster_panel, slot_degree, slot_offset, panels, psw, amat,
-                                     amat_off, ucos_all, ucos_off, S4);
+                                     amat_off, ucos_all, ucos_off, used, S4);
   count_launch();
   return cudaGetLastError();
 }
@@ -311,11 +314,11 @@ cudaError_t launch_resolve(int dim, int n_pc, const int* pc_entry, const int* pc
                            const int* cluster_slot_begin_s, const long long* tgt_slot_offset,
                            const int* cluster_slot_begin_t, int slot_d_lo, long long t4_base, long long s4_base,
                            const double* tgt_centre, int n_point_items, WorkItem* items, Entry* entries,
-                           int far_item0, int far_entry0, cudaStream_t s) {
+                           int far_item0, int far_entry0, int* slot_used, cudaStream_t s) {
   if (n_pc > 0) {
     k_resolve_pc<<<(n_pc + 255) / 256, 256, 0, s>>>(dim, n_pc, pc_entry, pc_src_cluster, deg_pc, pc_direct,
                                                     src_slot_offset, cluster_slot_begin_s, slot_d_lo, s4_base,
-                                                    entries);
+                                                    entries, slot_used);
     count_launch();
   }
   if (n_point_items > 0) {
@@ -326,7 +329,7 @@ cudaError_t launch_resolve(int dim, int n_pc, const int* pc_entry, const int* pc
     k_far_items<<<(n_far + 127) / 128, 128, 0, s>>>(dim, n_far, tiles_max, far_type, far_tgt_cluster, far_src, deg_far,
                                                     tgt_slot_offset, cluster_slot_begin_t, src_slot_offset,
                                                     cluster_slot_begin_s, slot_d_lo, t4_base, s4_base, tgt_centre,
-                                                    items, entries, far_item0, far_entry0);
+                                                    items, entries, far_item0, far_entry0, slot_used);
     count_launch();
   }
   return cudaGetLastError();

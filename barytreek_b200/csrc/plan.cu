@@ -661,6 +661,7 @@ struct btk_plan {
   int n_src_slots = 0, n_tgt_slots = 0;
   long long total_src_slots = 0, total_tgt_slots = 0;
   int *d_s_slot_panel = nullptr, *d_s_slot_deg = nullptr, *d_s_cluster_slot_begin = nullptr;
+  int* d_s_slot_used = nullptr;  // per source slot: read by this solve's work items
   int *d_t_slot_deg = nullptr, *d_t_cluster_slot_begin = nullptr, *d_t_cluster_panel = nullptr;
   long long *d_s_slot_off = nullptr, *d_t_slot_off = nullptr;
   double* d_amat = nullptr;
@@ -858,6 +859,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   BTK_TRY(A.upload(&P->d_ucos, ucos));
   BTK_TRY(A.upload(&P->d_ucos_off, ucos_off));
   BTK_TRY(A.upload(&P->d_s_slot_panel, s_panel));
+  BTK_TRY(A.alloc(&P->d_s_slot_used, (size_t)std::max(P->n_src_slots, 1)));
   BTK_TRY(A.upload(&P->d_s_slot_deg, s_deg));
   BTK_TRY(A.upload(&P->d_s_slot_off, s_off));
   BTK_TRY(A.upload(&P->d_s_cluster_slot_begin, s_begin));
@@ -1256,17 +1258,18 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
     BTK_CUDA(launch_src_proxies(P->dim, P->degree, (int)S.clusters.size(), S.d_clusters, S.d_nodes_shift, P->d_psw,
                                 P->d_S4 + S.n_points, st));
   } else {
-    // Every source cluster at every slot degree, then the work items for the
-    // degrees in force.
-    BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
-                              S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
-                              P->d_S4 + S.n_points, st));
+    // Work items for the degrees in force (marking the source slots they
+    // read), then those slots.
+    BTK_CUDA(cudaMemsetAsync(P->d_s_slot_used, 0, sizeof(int) * (size_t)std::max(P->n_src_slots, 1), st));
     BTK_CUDA(launch_resolve(P->dim, P->n_pc, P->d_pc_entry, P->d_pc_src_cluster, P->d_deg_pc, P->d_pc_direct,
                             P->n_far, P->tiles_max,
                             P->d_far_type, P->d_far_tgt, P->d_far_src, P->d_deg_far, P->d_s_slot_off,
                             P->d_s_cluster_slot_begin, P->d_t_slot_off, P->d_t_cluster_slot_begin, P->degree_min,
                             T.n_points, S.n_points, P->d_tgt_centre, P->n_static_items, P->ictx.d_items,
-                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, st));
+                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, P->d_s_slot_used, st));
+    BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
+                              S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
+                              P->d_s_slot_used, P->d_S4 + S.n_points, st));
   }
   BTK_CUDA(cudaEventRecord(P->ev[1], st));
   // Interactions.
@@ -1556,15 +1559,18 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   BTK_CUDA(cudaEventRecord(ek[1], st));
   bool first = true;
   auto solve = [&](const InteractCtx& ctx) -> btk_status {
-    BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
-                              S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
-                              P->d_S4 + S.n_points, st));
+    // Work items for the degrees in force (marking the source slots they
+    // read), then those slots.
+    BTK_CUDA(cudaMemsetAsync(P->d_s_slot_used, 0, sizeof(int) * (size_t)std::max(P->n_src_slots, 1), st));
     BTK_CUDA(launch_resolve(P->dim, P->n_pc, P->d_pc_entry, P->d_pc_src_cluster, P->d_deg_pc, P->d_pc_direct,
                             P->n_far, P->tiles_max,
                             P->d_far_type, P->d_far_tgt, P->d_far_src, P->d_deg_far, P->d_s_slot_off,
                             P->d_s_cluster_slot_begin, P->d_t_slot_off, P->d_t_cluster_slot_begin, P->degree_min,
                             T.n_points, S.n_points, P->d_tgt_centre, P->n_static_items, P->ictx.d_items,
-                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, st));
+                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, P->d_s_slot_used, st));
+    BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
+                              S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
+                              P->d_s_slot_used, P->d_S4 + S.n_points, st));
     BTK_CUDA(launch_gather(T.n_points, T.d_perm, xt, yt, P->dim == 3 ? zt : nullptr, nullptr, P->d_T4, st));
     BTK_CUDA(cudaMemsetAsync(P->d_ptw, 0, sizeof(double) * (size_t)P->ncomp * Pt * P->ipc, st));
     BTK_CUDA(cudaMemsetAsync(P->d_ptwm, 0, sizeof(double) * (size_t)P->ncomp * P->total_tgt_slots, st));
@@ -1666,7 +1672,7 @@ btk_status btk_plan_error_samples(btk_plan* P, const double* xt, const double* y
   BTK_CUDA(cudaMemsetAsync(P->d_psw, 0, sizeof(double) * (size_t)S.h.panel_count * P->ipc, st));
   BTK_TRY(run_upward(S, P->d_S4, P->d_psw, st));
   BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
-                            S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
+                            S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off, nullptr,
                             P->d_S4 + S.n_points, st));
   Arena A(st);
   int *d_pi = nullptr, *d_to = nullptr, *d_csr = nullptr, *d_sl = nullptr;
