@@ -27,6 +27,7 @@
 // fewer pairs run at PT/2 or PT/4. Results are added to the proxy target
 // weights with FP64 atomics (pairs of one target panel sit in many groups).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <tuple>
@@ -269,12 +270,19 @@ cudaError_t launch_cc_one(const CcParams& p, int t0, int t1, cudaStream_t s) {
   constexpr int NC = CcTraits<DIM, KIND>::NC;
   const size_t smem = cc_smem_bytes(DIM, NC, p.m, PT, F32);
   const dim3 grid(t1 - t0, (p.ipc + kCcJ - 1) / kCcJ);
-  // The shared-memory opt-in is set once per kernel (for the largest degree),
-  // outside any stream capture a caller may have open at later launches.
-  static const cudaError_t attr =
-      cudaFuncSetAttribute(k_cc_groups<DIM, KIND, PT, GUARD, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)cc_smem_bytes(DIM, NC, kMaxNodes, PT, F32));
-  if (attr != cudaSuccess) return attr;
+  // The shared-memory opt-in is set once per kernel and device (for the
+  // largest degree), at the first launch there.
+  static std::atomic<uint64_t> opted{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(opted.load(std::memory_order_acquire) & bit)) {
+    e = cudaFuncSetAttribute(k_cc_groups<DIM, KIND, PT, GUARD, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)cc_smem_bytes(DIM, NC, kMaxNodes, PT, F32));
+    if (e != cudaSuccess) return e;
+    opted.fetch_or(bit, std::memory_order_release);
+  }
   k_cc_groups<DIM, KIND, PT, GUARD, F32><<<grid, kCcJ, smem, s>>>(p, t0);
   count_launch();
   return cudaGetLastError();
