@@ -186,12 +186,19 @@ cudaError_t launch_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, int c
                                        int* deg, cudaStream_t s);
 cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, int lo, int hi, int dim, int conv0,
                                   int n_pc, const int* pc_direct, int* deg, cudaStream_t s);
+// The form of each leaf pair k < n (direct, PC entry pc0 + k, or for k < n_cc
+// CC entry cc0 + k) and its degree; cost_rule as BTK_DEGREE_RULE_COST.
+cudaError_t launch_choose_leaf_pairs(int n, int n_cc, int dim, int pc0, int cc0, const float* pred, float log10_target,
+                                     int lo, int hi, int cost_rule, const int* pc_tcount, const int* pc_direct,
+                                     const int* weight, float inv_cbar, float inv_wbar, int* deg, cudaStream_t s);
 // Far-field evaluations at the chosen degrees (summed into evals[0]), direct
 // evaluations of the leaf pairs kept direct (evals[1]) and the histogram of
-// the degrees (hist[0..12], added to).
-cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
-                             const int* cp_scount, const int* pc_direct, unsigned long long* evals, int* hist,
-                             cudaStream_t s);
+// the degrees (hist[0..12], added to; bin 0: leaf pairs kept direct). Leaf
+// pairs: PC entries [conv0, conv0 + n_conv), the first n_conv_cc with CC
+// entries, the last n_conv_cc of the CC block.
+cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, int conv0, int n_conv, int n_conv_cc,
+                             const int* deg, const int* pc_tcount, const int* cp_scount, const int* pc_direct,
+                             unsigned long long* evals, int* hist, cudaStream_t s);
 cudaError_t launch_audit_compare(int n, int ncomp, int nt, const int* audit_sorted, const int* perm,
                                  const double* out, const double* audit_out, double* sums, cudaStream_t s);
 cudaError_t launch_fill_int(int n, int value, int* dst, cudaStream_t s);

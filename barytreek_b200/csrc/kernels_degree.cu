@@ -201,7 +201,8 @@ __device__ __forceinline__ int ipow_d(int b, int dim) { return dim == 3 ? b * b 
 
 // Re-points the PC entries of point-target items at the chosen degree's slot.
 // Degree 0 (leaf pairs that may be approximated, kept direct): the source
-// leaf's points, pc_direct[2 i] (first) and [2 i + 1] (count).
+// leaf's points, pc_direct[2 i] (first) and [2 i + 1] (count); degree -1 (the
+// leaf pair's CC form taken instead): an empty entry.
 __global__ void k_resolve_pc(int dim, int n_pc, const int* pc_entry, const int* pc_src_cluster, const int* degree,
                              const int* pc_direct, const long long* src_slot_offset, const int* cluster_slot_begin_s,
                              int slot_d_lo, long long s4_base, Entry* entries, int* slot_used) {
@@ -209,7 +210,10 @@ __global__ void k_resolve_pc(int dim, int n_pc, const int* pc_entry, const int* 
   if (i >= n_pc) return;
   const int d = degree[i];
   Entry e;
-  if (d == 0) {
+  if (d < 0) {
+    e.s_begin = 0;
+    e.s_count = 0;
+  } else if (d == 0) {
     e.s_begin = pc_direct[2 * i];
     e.s_count = pc_direct[2 * i + 1];
   } else {
@@ -243,6 +247,15 @@ __global__ void k_far_items(int dim, int n_far, int tiles_max, const int* far_ty
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_far) return;
   const int d = degree[i];
+  if (d <= 0) {  // a leaf pair's CC form, not taken this solve: empty entry and tiles
+    entries[far_entry0 + i] = Entry{0, 0};
+    for (int k = 0; k < tiles_max; ++k) {
+      WorkItem w{};
+      w.e_begin = w.e_end = far_entry0 + i;
+      items[far_item0 + (size_t)i * tiles_max + k] = w;
+    }
+    return;
+  }
   const int ipc_d = ipow_d(d + 1, dim);
   Entry e;
   if (far_type[i] == 2) {  // CP: the source leaf's points (far_src packs begin, count)

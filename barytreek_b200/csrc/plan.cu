@@ -654,7 +654,8 @@ struct btk_plan {
   int n_pc = 0, n_cp = 0, n_far = 0, tiles_max = 0, n_static_items = 0, n_static_entries = 0;
   // Leaf pairs the degree choice may approximate (leaf_far_pairs): PC-block
   // pairs [n_pc_list, n_pc), degree 0 = direct.
-  int leaf_far = 0, n_pc_list = 0;
+  int leaf_far = 0, n_pc_list = 0, n_far_list = 0, n_tgt_slot_panels = 0;
+  int n_conv_cc = 0;  // leaf pairs with a CC form: the first of them, CC entries closing the far block
   double leaf_theta = 0.8;  // separation bound of the leaf pairs
   int64_t conv_direct_total = 0;  // their direct evaluations (all included in evals[0])
   int* d_pc_direct = nullptr;
@@ -745,7 +746,8 @@ void recount_far_evals(btk_plan* P) {
   for (int i = 0; i < P->n_pc; ++i)
     if (P->h_deg_pc[i] > 0) P->evals[1] += P->h_pc_tcount[i] * sz(P->h_deg_pc[i]);
   for (int i = 0; i < P->n_cp; ++i) P->evals[2] += sz(P->h_deg_far[i]) * P->h_cp_scount[i];
-  for (int i = P->n_cp; i < P->n_far; ++i) P->evals[3] += sz(P->h_deg_far[i]) * sz(P->h_deg_far[i]);
+  for (int i = P->n_cp; i < P->n_far; ++i)
+    if (P->h_deg_far[i] > 0) P->evals[3] += sz(P->h_deg_far[i]) * sz(P->h_deg_far[i]);
 }
 
 // The audit's targets and work items (built on the host; see build_audit_work).
@@ -793,6 +795,9 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   std::vector<int> conv;                         // PP pair indices
   std::vector<int> slot_panels_s(S.clusters);    // source panels with degree slots
   std::vector<int> slot_of_s(S.cluster_slot);    // per source panel: its index there (-1: none)
+  std::vector<int> slot_panels_t(T.clusters);    // target panels with degree slots
+  std::vector<int> slot_of_t(T.cluster_slot);
+  int n_conv_cc = 0;
   if (P->leaf_far) {
     for (int i = 0; i < counts[0]; ++i) {
       const btk_interact_pair& pr = lists[0][i];
@@ -819,18 +824,33 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
       if (dist > 0 && gap > 0.5 * side && (0.5 * std::sqrt(ra) + 0.5 * std::sqrt(rb)) / dist < P->leaf_theta)
         conv.push_back(i);
     }
+    // Pairs whose target leaf holds more points than the plan degree's
+    // proxies also get a CC form (target-leaf proxies x source-leaf proxies,
+    // cheaper than the PC form at every degree): they go first, and their
+    // target leaves get degree slots after the clusters'.
+    std::stable_partition(conv.begin(), conv.end(),
+                          [&](int i) { return T.h.point_count[lists[0][i].target_panel] > sz(n); });
     for (int i : conv) {
-      const int sp = lists[0][i].source_panel;
+      const int sp = lists[0][i].source_panel, tp = lists[0][i].target_panel;
       if (slot_of_s[sp] < 0) {
         slot_of_s[sp] = (int)slot_panels_s.size();
         slot_panels_s.push_back(sp);
+      }
+      if (T.h.point_count[tp] > sz(n)) {
+        ++n_conv_cc;
+        if (slot_of_t[tp] < 0) {
+          slot_of_t[tp] = (int)slot_panels_t.size();
+          slot_panels_t.push_back(tp);
+        }
       }
     }
   }
   std::vector<int> s_panel, s_deg, s_begin, t_panel, t_deg, t_begin;
   std::vector<long long> s_off, t_off;
   P->total_src_slots = make_slots(slot_panels_s, s_panel, s_deg, s_off, s_begin);
-  P->total_tgt_slots = make_slots(T.clusters, t_panel, t_deg, t_off, t_begin);
+  P->total_tgt_slots = make_slots(slot_panels_t, t_panel, t_deg, t_off, t_begin);
+  P->n_tgt_slot_panels = (int)slot_panels_t.size();
+  P->n_conv_cc = n_conv_cc;
   P->n_src_slots = (int)s_panel.size();
   P->n_tgt_slots = (int)t_panel.size();
   BTK_CHECK(S.n_points + P->total_src_slots < (1LL << 31) && T.n_points + P->total_tgt_slots < (1LL << 31),
@@ -866,7 +886,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   BTK_TRY(A.upload(&P->d_t_slot_deg, t_deg));
   BTK_TRY(A.upload(&P->d_t_slot_off, t_off));
   BTK_TRY(A.upload(&P->d_t_cluster_slot_begin, t_begin));
-  BTK_TRY(A.upload(&P->d_t_cluster_panel, T.clusters));
+  BTK_TRY(A.upload(&P->d_t_cluster_panel, slot_panels_t));
 
   // Static items: PP and PC (PC entries start at the degree-n slot). The PC
   // block of the per-pair arrays is the PC list, then the leaf pairs (their
@@ -874,7 +894,8 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   P->n_pc_list = counts[1];
   P->n_pc = counts[1] + (int)conv.size();
   P->n_cp = counts[2];
-  P->n_far = counts[2] + counts[3];
+  P->n_far_list = counts[2] + counts[3];
+  P->n_far = P->n_far_list + n_conv_cc;  // the leaf pairs' CC forms close the far block
   std::vector<long long> pc_begin(P->n_pc_list);
   std::vector<int> pc_src_cluster(P->n_pc), pc_direct(2 * (size_t)std::max(P->n_pc, 1), -1);
   P->h_pc_tcount.resize(P->n_pc);
@@ -915,7 +936,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   // Far pairs: CP then CC.
   std::vector<int> far_type(P->n_far), far_tgt(P->n_far), far_src(2 * (size_t)P->n_far);
   P->h_cp_scount.resize(P->n_cp);
-  for (int i = 0; i < P->n_far; ++i) {
+  for (int i = 0; i < P->n_far_list; ++i) {
     const bool cp = i < P->n_cp;
     const btk_interact_pair& pr = cp ? lists[2][i] : lists[3][i - P->n_cp];
     BTK_CHECK(pr.target_panel >= 0 && pr.target_panel < T.h.panel_count && pr.source_panel >= 0 &&
@@ -935,10 +956,19 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
       far_src[2 * i + 1] = 0;
     }
   }
-  std::vector<double> centre(3 * (size_t)std::max(nct, 1), 0.0);
-  for (int c = 0; c < nct; ++c)
+  for (int k = 0; k < n_conv_cc; ++k) {
+    const btk_interact_pair& pr = lists[0][conv[k]];
+    const int i = P->n_far_list + k;
+    far_type[i] = 3;
+    far_tgt[i] = slot_of_t[pr.target_panel];
+    far_src[2 * i] = slot_of_s[pr.source_panel];
+    far_src[2 * i + 1] = 0;
+  }
+  const int n_tsp = P->n_tgt_slot_panels;
+  std::vector<double> centre(3 * (size_t)std::max(n_tsp, 1), 0.0);
+  for (int c = 0; c < n_tsp; ++c)
     for (int d = 0; d < 3; ++d) {
-      const PanelGeom& g = T.h.geom[T.clusters[c]];
+      const PanelGeom& g = T.h.geom[slot_panels_t[c]];
       centre[3 * c + d] = 0.5 * (g.lo[d] + g.hi[d]);
     }
   P->tiles_max = (int)((sz(n) + kTile - 1) / kTile);
@@ -969,10 +999,12 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   P->h_deg_pc.assign(P->n_pc, n);
   std::fill(P->h_deg_pc.begin() + P->n_pc_list, P->h_deg_pc.end(), 0);  // leaf pairs: direct
   P->h_deg_far.assign(P->n_far, n);
+  std::fill(P->h_deg_far.begin() + P->n_far_list, P->h_deg_far.end(), 0);  // leaf pairs' CC forms: not taken
   P->n_pairs = P->n_pc + P->n_far;
   {
     std::vector<int> all(std::max(P->n_pairs, 1), n);
     std::fill(all.begin() + P->n_pc_list, all.begin() + P->n_pc, 0);
+    std::fill(all.begin() + P->n_pc + P->n_far_list, all.begin() + P->n_pairs, 0);
     BTK_TRY(A.upload(&P->d_deg_pc, all));  // one array: PC (list, leaf pairs) degrees, then CP, then CC
     P->d_deg_far = P->d_deg_pc + P->n_pc;
   }
@@ -988,7 +1020,8 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     }
     for (int i = 0; i < P->n_far; ++i) {
       const bool cp = i < P->n_cp;
-      const btk_interact_pair& pr = cp ? lists[2][i] : lists[3][i - P->n_cp];
+      const btk_interact_pair& pr =
+          cp ? lists[2][i] : (i < P->n_far_list ? lists[3][i - P->n_cp] : lists[0][conv[i - P->n_far_list]]);
       ty[P->n_pc + i] = cp ? 2 : 3;
       tg[P->n_pc + i] = pr.target_panel;
       sr[P->n_pc + i] = pr.source_panel;
@@ -1023,7 +1056,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     BTK_TRY(A.alloc(&P->d_evals, 2));
     BTK_TRY(A.alloc(&P->d_gsum, 2));
     BTK_TRY(A.upload(&P->d_cluster_slot_s, slot_of_s));
-    BTK_TRY(A.upload(&P->d_cluster_slot_t, T.cluster_slot));
+    BTK_TRY(A.upload(&P->d_cluster_slot_t, slot_of_t));
     const PanelGeom& g = S.h.geom[0];
     double r2 = 0;
     for (int d = 0; d < dim; ++d) {
@@ -1303,7 +1336,7 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
                               P->cc_bucket_end, st));
   }
   if (per_pair)
-    BTK_CUDA(launch_promote(P->dim, P->degree, P->ncomp, (int)T.clusters.size(), P->d_t_cluster_panel,
+    BTK_CUDA(launch_promote(P->dim, P->degree, P->ncomp, P->n_tgt_slot_panels, P->d_t_cluster_panel,
                             P->d_t_cluster_slot_begin, P->d_t_slot_deg, P->d_t_slot_off, P->d_amat, P->d_amat_off,
                             wm, w, st));
   BTK_CUDA(cudaEventRecord(P->ev[2], st));
@@ -1543,8 +1576,13 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
                                    P->n_pc_list, P->n_pc, P->d_pc_direct, P->d_deg_pc, st));
   BTK_CUDA(cudaMemsetAsync(P->d_evals, 0, 2 * sizeof(unsigned long long), st));
   BTK_CUDA(cudaMemsetAsync(P->d_report, 0, sizeof(int) * kMaxNodes, st));
-  BTK_CUDA(launch_far_evals(P->dim, P->n_pc, P->n_cp, P->n_far - P->n_cp, P->d_deg_pc, P->d_pc_tcount,
-                            P->d_cp_scount, P->d_pc_direct, P->d_evals, P->d_report, st));
+  BTK_CUDA(launch_choose_leaf_pairs(P->n_pc - P->n_pc_list, P->n_conv_cc, P->dim, P->n_pc_list,
+                                    P->n_pc + P->n_far_list, P->d_pred, (float)std::log10(pair_tol), lo, P->degree,
+                                    P->degree_rule == BTK_DEGREE_RULE_COST ? 1 : 0, P->d_pc_tcount, P->d_pc_direct,
+                                    P->d_pair_weight, P->inv_cbar, P->inv_wbar, P->d_deg_pc, st));
+  BTK_CUDA(launch_far_evals(P->dim, P->n_pc, P->n_cp, P->n_far - P->n_cp, P->n_pc_list, P->n_pc - P->n_pc_list,
+                            P->n_conv_cc, P->d_deg_pc, P->d_pc_tcount, P->d_cp_scount, P->d_pc_direct, P->d_evals,
+                            P->d_report, st));
   BTK_CUDA(cudaEventRecord(e[1], st));
   // Solve at the chosen degrees.
   Ptr4 o{}, w{}, wm{};
@@ -1578,7 +1616,7 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     BTK_TRY(run_interactions(ctx, P->d_S4, P->d_T4, P->d_T_out, o, wm, st, first ? ek[0] : nullptr,
                              first ? ek[1] : nullptr));
     first = false;
-    BTK_CUDA(launch_promote(P->dim, P->degree, P->ncomp, (int)T.clusters.size(), P->d_t_cluster_panel,
+    BTK_CUDA(launch_promote(P->dim, P->degree, P->ncomp, P->n_tgt_slot_panels, P->d_t_cluster_panel,
                             P->d_t_cluster_slot_begin, P->d_t_slot_deg, P->d_t_slot_off, P->d_amat, P->d_amat_off,
                             wm, w, st));
     BTK_TRY(run_downward(T, P->ncomp, P->d_T4, w, o, st));
@@ -1618,6 +1656,7 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     fell_back = 1;
     BTK_CUDA(launch_fill_int(P->n_pairs, P->degree, P->d_deg_pc, st));
     BTK_CUDA(launch_fill_int(P->n_pc - P->n_pc_list, 0, P->d_deg_pc + P->n_pc_list, st));
+    BTK_CUDA(launch_fill_int(P->n_far - P->n_far_list, 0, P->d_deg_pc + P->n_pc + P->n_far_list, st));
     InteractCtx plain = P->ictx;
     plain.precision = BTK_PREC_FP64;
     BTK_TRY(solve(plain));
@@ -1745,7 +1784,7 @@ btk_status btk_plan_set_degrees(btk_plan* P, const int* deg_pc, const int* deg_c
       if (v[i] < lo || v[i] > hi) return false;
     return true;
   };
-  const int n_cc = P->n_far - P->n_cp;
+  const int n_cc = P->n_far_list - P->n_cp;  // the CC list (leaf pairs stay direct)
   BTK_CHECK(!deg_pc || check(deg_pc, P->n_pc_list), BTK_ERR_INVALID_ARGUMENT,
             "PC degree outside [degree_min, degree]");
   BTK_CHECK(!deg_cp || check(deg_cp, P->n_cp), BTK_ERR_INVALID_ARGUMENT, "CP degree outside [degree_min, degree]");

@@ -491,24 +491,87 @@ __global__ void k_choose_degrees_cost(int n, int dim, int n_pc, int n_cp, int co
   deg[i] = d_best;
 }
 
+// Leaf pairs k < n (the PP pairs the degree choice may approximate): one
+// decision over the direct evaluation, target points x source-leaf proxies
+// (PC entry pc0 + k) and, for k < n_cc (target leaves with more points than
+// the plan degree's proxies), target-leaf proxies x source-leaf proxies (CC
+// entry cc0 + k), each approximation at its own predicted errors. Cost rule:
+// the least cost / mean cost + (w / mean w) (err / pair_tol)^2, direct at its
+// cost and no error; threshold rule: the cheapest form meeting the pair
+// tolerance (direct always does). Degrees written: direct = PC entry 0 (its
+// entry is the source leaf's points), CC entry 0 (no items); PC form = PC
+// entry d, CC entry 0; CC form = PC entry -1 (empty entry), CC entry d.
+__global__ void k_choose_leaf_pairs(int n, int n_cc, int dim, int pc0, int cc0, const float* pred,
+                                    float log10_target, int lo, int hi, int cost_rule, const int* pc_tcount,
+                                    const int* pc_direct, const int* weight, float inv_cbar, float inv_wbar,
+                                    int* deg) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int i = pc0 + k, j = cc0 + k;
+  const bool has_cc = k < n_cc;
+  const float nt = (float)pc_tcount[i], ns = (float)pc_direct[2 * i + 1];
+  const float wr = (float)weight[i] * inv_wbar;
+  float best = cost_rule ? nt * ns * inv_cbar : nt * ns;
+  int form = 0, d_best = 0;
+  for (int c = max(lo, kDegLo); c <= hi && c < kDegLo + kO; ++c) {
+    const float m = (float)(c + 1);
+    const float md = dim == 3 ? m * m * m : m * m;
+    const float p_pc = pred[(size_t)i * kO + (c - kDegLo)];
+    const float p_cc = has_cc ? pred[(size_t)j * kO + (c - kDegLo)] : 3.4e38f;
+    float j_pc, j_cc = 3.4e38f;
+    if (cost_rule) {
+      const float e_pc = exp10f(fminf(p_pc - log10_target, 18.f));
+      j_pc = nt * md * inv_cbar + wr * e_pc * e_pc;
+      if (has_cc) {
+        const float e_cc = exp10f(fminf(p_cc - log10_target, 18.f));
+        j_cc = md * md * inv_cbar + wr * e_cc * e_cc;
+      }
+    } else {
+      j_pc = p_pc <= log10_target ? nt * md : 3.4e38f;
+      if (has_cc && p_cc <= log10_target) j_cc = md * md;
+    }
+    if (j_pc < best) {
+      best = j_pc;
+      form = 1;
+      d_best = c;
+    }
+    if (j_cc < best) {
+      best = j_cc;
+      form = 2;
+      d_best = c;
+    }
+  }
+  deg[i] = form == 1 ? d_best : (form == 2 ? -1 : 0);
+  if (has_cc) deg[j] = form == 2 ? d_best : 0;
+}
+
 // Far-field evaluations at the chosen degrees (pairs PC, CP, CC in order) into
-// evals[0]; leaf pairs kept direct (degree 0) add their direct evaluations to
-// evals[1].
-__global__ void k_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
-                            const int* cp_scount, const int* pc_direct, unsigned long long* evals, int* hist) {
+// evals[0]. Leaf pairs: PC entries [conv0, conv0 + n_conv), the first n_conv_cc
+// of them with a CC entry among the last n_conv_cc of the CC block; a leaf pair
+// kept direct (PC entry 0 and no CC form taken) adds its direct evaluations to
+// evals[1] and counts in histogram bin 0; entries at degree <= 0 (forms not
+// taken) count nowhere.
+__global__ void k_far_evals(int dim, int n_pc, int n_cp, int n_cc, int conv0, int n_conv, int n_conv_cc,
+                            const int* deg, const int* pc_tcount, const int* cp_scount, const int* pc_direct,
+                            unsigned long long* evals, int* hist) {
   __shared__ int sh[kMaxDegree + 1];
   if (threadIdx.x <= kMaxDegree) sh[threadIdx.x] = 0;
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long v = 0, vd = 0;
   const int n = n_pc + n_cp + n_cc;
-  if (i < n && deg[i] >= 0 && deg[i] <= kMaxDegree) atomicAdd(&sh[deg[i]], 1);
-  if (i < n) {
+  const int cc_leaf0 = n - n_conv_cc;
+  bool counted = i < n && deg[i] > 0 && deg[i] <= kMaxDegree;
+  if (i < n && deg[i] == 0 && i >= conv0 && i < conv0 + n_conv &&
+      (i - conv0 >= n_conv_cc || deg[cc_leaf0 + (i - conv0)] == 0)) {
+    counted = true;  // leaf pair kept direct
+    vd = (unsigned long long)pc_tcount[i] * (unsigned long long)pc_direct[2 * i + 1];
+  }
+  if (counted) atomicAdd(&sh[deg[i]], 1);
+  if (i < n && deg[i] > 0) {
     const unsigned long long m = (unsigned long long)(deg[i] + 1);
     const unsigned long long s = dim == 3 ? m * m * m : m * m;
-    if (i < n_pc && deg[i] == 0)
-      vd = (unsigned long long)pc_tcount[i] * (unsigned long long)pc_direct[2 * i + 1];
-    else if (i < n_pc)
+    if (i < n_pc)
       v = s * (unsigned long long)pc_tcount[i];
     else if (i < n_pc + n_cp)
       v = s * (unsigned long long)cp_scount[i - n_pc];
@@ -737,13 +800,13 @@ __global__ void k_fill_int(int n, int value, int* dst) {
 // ---- launchers -----------------------------------------------------------------
 int selector_param_count() { return kParams; }
 
-cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, const int* deg, const int* pc_tcount,
-                             const int* cp_scount, const int* pc_direct, unsigned long long* evals, int* hist,
-                             cudaStream_t s) {
+cudaError_t launch_far_evals(int dim, int n_pc, int n_cp, int n_cc, int conv0, int n_conv, int n_conv_cc,
+                             const int* deg, const int* pc_tcount, const int* cp_scount, const int* pc_direct,
+                             unsigned long long* evals, int* hist, cudaStream_t s) {
   const int n = n_pc + n_cp + n_cc;
   if (n <= 0) return cudaSuccess;
-  k_far_evals<<<(n + 255) / 256, 256, 0, s>>>(dim, n_pc, n_cp, n_cc, deg, pc_tcount, cp_scount, pc_direct, evals,
-                                              hist);
+  k_far_evals<<<(n + 255) / 256, 256, 0, s>>>(dim, n_pc, n_cp, n_cc, conv0, n_conv, n_conv_cc, deg, pc_tcount,
+                                              cp_scount, pc_direct, evals, hist);
   count_launch();
   return cudaGetLastError();
 }
@@ -824,6 +887,16 @@ cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const
   const int tiles = (n + 15) / 16;
   const int grid = std::max(1, std::min((tiles + 3) / 4, 8 * sms));
   k_mlp_infer<<<grid, 128, 0, s>>>(n, (const __nv_bfloat16*)w_bf16, nrm, feat, out);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_choose_leaf_pairs(int n, int n_cc, int dim, int pc0, int cc0, const float* pred, float log10_target,
+                                     int lo, int hi, int cost_rule, const int* pc_tcount, const int* pc_direct,
+                                     const int* weight, float inv_cbar, float inv_wbar, int* deg, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_choose_leaf_pairs<<<(n + 255) / 256, 256, 0, s>>>(n, n_cc, dim, pc0, cc0, pred, log10_target, lo, hi, cost_rule,
+                                                      pc_tcount, pc_direct, weight, inv_cbar, inv_wbar, deg);
   count_launch();
   return cudaGetLastError();
 }

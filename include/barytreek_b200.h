@@ -347,7 +347,9 @@ typedef struct {
    * is cheaper as target points x source proxies when the source leaf has more
    * than (d+1)^dim points. Such pairs join the PC pairs of the degree choice,
    * with the direct evaluation as one more option (chosen when it is cheaper
-   * or when no degree meets the pair tolerance under the cost rule); the
+   * or when no degree meets the pair tolerance under the cost rule), and,
+   * where the target leaf holds more points than the plan degree's proxies,
+   * target-leaf proxies x source-leaf proxies as a third; the
    * fallback and btk_plan_execute evaluate them directly, as the reference
    * does. 0: PP pairs are always direct. */
   int leaf_far_pairs;
