@@ -545,6 +545,49 @@ __global__ void k_choose_leaf_pairs(int n, int n_cc, int dim, int pc0, int cc0, 
   if (has_cc) deg[j] = form == 2 ? d_best : 0;
 }
 
+// PC pairs whose target leaf holds more points than the plan degree's proxies
+// (k < n): the PC form (entry pc_idx[k]) or target-leaf proxies x
+// source-cluster proxies (CC entry cc0 + k), each at its own degrees, by the
+// same rules (threshold rule with no form meeting the tolerance: PC at hi).
+// The form not taken gets degree -1 (PC entry) or 0 (CC entry).
+__global__ void k_choose_pc_cc(int n, int dim, const int* pc_idx, int cc0, const float* pred, float log10_target,
+                               int lo, int hi, int cost_rule, const int* pc_tcount, const int* weight, float inv_cbar,
+                               float inv_wbar, int* deg) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int i = pc_idx[k], j = cc0 + k;
+  const float nt = (float)pc_tcount[i];
+  const float wr = (float)weight[i] * inv_wbar;
+  float best = 3.4e38f;
+  int form = 1, d_best = hi;
+  for (int c = max(lo, kDegLo); c <= hi && c < kDegLo + kO; ++c) {
+    const float m = (float)(c + 1);
+    const float md = dim == 3 ? m * m * m : m * m;
+    const float p_pc = pred[(size_t)i * kO + (c - kDegLo)], p_cc = pred[(size_t)j * kO + (c - kDegLo)];
+    float j_pc, j_cc;
+    if (cost_rule) {
+      const float e_pc = exp10f(fminf(p_pc - log10_target, 18.f)), e_cc = exp10f(fminf(p_cc - log10_target, 18.f));
+      j_pc = nt * md * inv_cbar + wr * e_pc * e_pc;
+      j_cc = md * md * inv_cbar + wr * e_cc * e_cc;
+    } else {
+      j_pc = p_pc <= log10_target ? nt * md : 3.4e38f;
+      j_cc = p_cc <= log10_target ? md * md : 3.4e38f;
+    }
+    if (j_pc < best) {
+      best = j_pc;
+      form = 1;
+      d_best = c;
+    }
+    if (j_cc < best) {
+      best = j_cc;
+      form = 2;
+      d_best = c;
+    }
+  }
+  deg[i] = form == 1 ? d_best : -1;
+  deg[j] = form == 2 ? d_best : 0;
+}
+
 // Far-field evaluations at the chosen degrees (pairs PC, CP, CC in order) into
 // evals[0]. Leaf pairs: PC entries [conv0, conv0 + n_conv), the first n_conv_cc
 // of them with a CC entry among the last n_conv_cc of the CC block; a leaf pair
@@ -897,6 +940,16 @@ cudaError_t launch_choose_leaf_pairs(int n, int n_cc, int dim, int pc0, int cc0,
   if (n <= 0) return cudaSuccess;
   k_choose_leaf_pairs<<<(n + 255) / 256, 256, 0, s>>>(n, n_cc, dim, pc0, cc0, pred, log10_target, lo, hi, cost_rule,
                                                       pc_tcount, pc_direct, weight, inv_cbar, inv_wbar, deg);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_choose_pc_cc(int n, int dim, const int* pc_idx, int cc0, const float* pred, float log10_target,
+                                int lo, int hi, int cost_rule, const int* pc_tcount, const int* weight,
+                                float inv_cbar, float inv_wbar, int* deg, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_choose_pc_cc<<<(n + 255) / 256, 256, 0, s>>>(n, dim, pc_idx, cc0, pred, log10_target, lo, hi, cost_rule,
+                                                 pc_tcount, weight, inv_cbar, inv_wbar, deg);
   count_launch();
   return cudaGetLastError();
 }
