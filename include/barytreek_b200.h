@@ -349,7 +349,8 @@ typedef struct {
    * with the direct evaluation as one more option (chosen when it is cheaper
    * or when no degree meets the pair tolerance under the cost rule), and,
    * where the target leaf holds more points than the plan degree's proxies,
-   * target-leaf proxies x source-leaf proxies as a third; the
+   * target-leaf proxies x source-leaf proxies as a third (the PC pairs of
+   * such target leaves get that form as their alternative too); the
    * fallback and btk_plan_execute evaluate them directly, as the reference
    * does. 0: PP pairs are always direct. */
   int leaf_far_pairs;
