@@ -191,11 +191,12 @@ cudaError_t launch_choose_degrees(int n, const float* pred, float log10_target, 
 cudaError_t launch_choose_leaf_pairs(int n, int n_cc, int dim, int pc0, int cc0, const float* pred, float log10_target,
                                      int lo, int hi, int cost_rule, const int* pc_tcount, const int* pc_direct,
                                      const int* weight, float inv_cbar, float inv_wbar, int* deg, cudaStream_t s);
-// PC pairs with a large target leaf, k < n: the PC form (entry pc_idx[k]) or
-// the CC form (entry cc0 + k) and its degree.
-cudaError_t launch_choose_pc_cc(int n, int dim, const int* pc_idx, int cc0, const float* pred, float log10_target,
-                                int lo, int hi, int cost_rule, const int* pc_tcount, const int* weight,
-                                float inv_cbar, float inv_wbar, int* deg, cudaStream_t s);
+// PC pairs with a large target leaf or CP pairs with a large source leaf,
+// k < n: their own form (entry idx[k], cost coef[k] (d+1)^dim, degree
+// off_first when not taken) or the CC form (entry cc0 + k) and its degree.
+cudaError_t launch_choose_two_forms(int n, int dim, const int* idx, const int* coef, int off_first, int cc0,
+                                   const float* pred, float log10_target, int lo, int hi, int cost_rule,
+                                   const int* weight, float inv_cbar, float inv_wbar, int* deg, cudaStream_t s);
 // Far-field evaluations at the chosen degrees (summed into evals[0]), direct
 // evaluations of the leaf pairs kept direct (evals[1]) and the histogram of
 // the degrees (hist[0..12], added to; bin 0: leaf pairs kept direct). Leaf

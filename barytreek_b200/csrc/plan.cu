@@ -657,7 +657,9 @@ struct btk_plan {
   int leaf_far = 0, n_pc_list = 0, n_far_list = 0, n_tgt_slot_panels = 0;
   int n_conv_cc = 0;  // leaf pairs with a CC form: the first of them, CC entries closing the far block
   int n_pccc = 0;     // PC pairs with a CC form (large target leaf); their CC entries precede the leaf pairs'
-  int* d_pccc_pc = nullptr;  // their PC entries
+  int n_cpcc = 0;     // CP pairs with a CC form (large source leaf); their CC entries follow the PC pairs'
+  int *d_pccc_idx = nullptr, *d_pccc_coef = nullptr;  // their PC entries, target leaf points
+  int *d_cpcc_idx = nullptr, *d_cpcc_coef = nullptr;  // their CP entries (pair array), source leaf points
   double leaf_theta = 0.8;  // separation bound of the leaf pairs
   int64_t conv_direct_total = 0;  // their direct evaluations (all included in evals[0])
   int* d_pc_direct = nullptr;
@@ -800,7 +802,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   std::vector<int> slot_panels_t(T.clusters);    // target panels with degree slots
   std::vector<int> slot_of_t(T.cluster_slot);
   int n_conv_cc = 0;
-  std::vector<int> pccc;  // PC-list pairs with a CC form
+  std::vector<int> pccc, cpcc;  // PC / CP list pairs with a CC form
   if (P->leaf_far) {
     for (int i = 0; i < counts[0]; ++i) {
       const btk_interact_pair& pr = lists[0][i];
@@ -859,6 +861,18 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
         slot_panels_t.push_back(tp);
       }
     }
+    // And for CP pairs (target proxies x source leaf points) with a large
+    // source leaf, whose leaf then gets degree slots.
+    for (int i = 0; i < counts[2]; ++i) {
+      const int sp = lists[2][i].source_panel;
+      BTK_CHECK(sp >= 0 && sp < S.h.panel_count, BTK_ERR_INVALID_ARGUMENT, "interaction list: panel index out of range");
+      if (S.h.point_count[sp] <= sz(n)) continue;
+      cpcc.push_back(i);
+      if (slot_of_s[sp] < 0) {
+        slot_of_s[sp] = (int)slot_panels_s.size();
+        slot_panels_s.push_back(sp);
+      }
+    }
   }
   std::vector<int> s_panel, s_deg, s_begin, t_panel, t_deg, t_begin;
   std::vector<long long> s_off, t_off;
@@ -867,7 +881,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   P->n_tgt_slot_panels = (int)slot_panels_t.size();
   P->n_conv_cc = n_conv_cc;
   P->n_pccc = (int)pccc.size();
-  BTK_TRY(A.upload(&P->d_pccc_pc, pccc.empty() ? std::vector<int>{0} : pccc));
+  P->n_cpcc = (int)cpcc.size();
   P->n_src_slots = (int)s_panel.size();
   P->n_tgt_slots = (int)t_panel.size();
   BTK_CHECK(S.n_points + P->total_src_slots < (1LL << 31) && T.n_points + P->total_tgt_slots < (1LL << 31),
@@ -912,7 +926,8 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   P->n_pc = counts[1] + (int)conv.size();
   P->n_cp = counts[2];
   P->n_far_list = counts[2] + counts[3];
-  P->n_far = P->n_far_list + P->n_pccc + n_conv_cc;  // CC forms of PC pairs, then of leaf pairs, close the far block
+  // CC forms of PC pairs, of CP pairs, then of leaf pairs close the far block
+  P->n_far = P->n_far_list + P->n_pccc + P->n_cpcc + n_conv_cc;
   std::vector<long long> pc_begin(P->n_pc_list);
   std::vector<int> pc_src_cluster(P->n_pc), pc_direct(2 * (size_t)std::max(P->n_pc, 1), -1);
   P->h_pc_tcount.resize(P->n_pc);
@@ -982,9 +997,34 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     BTK_CHECK(far_src[2 * i] >= 0, BTK_ERR_INVALID_ARGUMENT, "PC pair with a leaf source");
     far_src[2 * i + 1] = 0;
   }
+  for (int k = 0; k < P->n_cpcc; ++k) {
+    const btk_interact_pair& pr = lists[2][cpcc[k]];
+    const int i = P->n_far_list + P->n_pccc + k;
+    far_type[i] = 3;
+    far_tgt[i] = T.cluster_slot[pr.target_panel];
+    BTK_CHECK(far_tgt[i] >= 0, BTK_ERR_INVALID_ARGUMENT, "CP pair with a leaf target");
+    far_src[2 * i] = slot_of_s[pr.source_panel];
+    far_src[2 * i + 1] = 0;
+  }
+  {
+    std::vector<int> ix(std::max<size_t>(pccc.size(), 1), 0), cf(ix.size(), 0);
+    for (size_t k = 0; k < pccc.size(); ++k) {
+      ix[k] = pccc[k];
+      cf[k] = T.h.point_count[lists[1][pccc[k]].target_panel];
+    }
+    BTK_TRY(A.upload(&P->d_pccc_idx, ix));
+    BTK_TRY(A.upload(&P->d_pccc_coef, cf));
+    std::vector<int> jx(std::max<size_t>(cpcc.size(), 1), 0), cg(jx.size(), 0);
+    for (size_t k = 0; k < cpcc.size(); ++k) {
+      jx[k] = P->n_pc + cpcc[k];  // CP entry in the pair array: after the PC block
+      cg[k] = S.h.point_count[lists[2][cpcc[k]].source_panel];
+    }
+    BTK_TRY(A.upload(&P->d_cpcc_idx, jx));
+    BTK_TRY(A.upload(&P->d_cpcc_coef, cg));
+  }
   for (int k = 0; k < n_conv_cc; ++k) {
     const btk_interact_pair& pr = lists[0][conv[k]];
-    const int i = P->n_far_list + P->n_pccc + k;
+    const int i = P->n_far_list + P->n_pccc + P->n_cpcc + k;
     far_type[i] = 3;
     far_tgt[i] = slot_of_t[pr.target_panel];
     far_src[2 * i] = slot_of_s[pr.source_panel];
@@ -1048,9 +1088,13 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
       const bool cp = i < P->n_cp;
       const btk_interact_pair& pr =
           cp ? lists[2][i]
-             : (i < P->n_far_list ? lists[3][i - P->n_cp]
-                                  : (i < P->n_far_list + P->n_pccc ? lists[1][pccc[i - P->n_far_list]]
-                                                                   : lists[0][conv[i - P->n_far_list - P->n_pccc]]));
+             : (i < P->n_far_list
+                    ? lists[3][i - P->n_cp]
+                    : (i < P->n_far_list + P->n_pccc
+                           ? lists[1][pccc[i - P->n_far_list]]
+                           : (i < P->n_far_list + P->n_pccc + P->n_cpcc
+                                  ? lists[2][cpcc[i - P->n_far_list - P->n_pccc]]
+                                  : lists[0][conv[i - P->n_far_list - P->n_pccc - P->n_cpcc]])));
       ty[P->n_pc + i] = cp ? 2 : 3;
       tg[P->n_pc + i] = pr.target_panel;
       sr[P->n_pc + i] = pr.source_panel;
@@ -1605,12 +1649,17 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
                                    P->n_pc_list, P->n_pc, P->d_pc_direct, P->d_deg_pc, st));
   BTK_CUDA(cudaMemsetAsync(P->d_evals, 0, 2 * sizeof(unsigned long long), st));
   BTK_CUDA(cudaMemsetAsync(P->d_report, 0, sizeof(int) * kMaxNodes, st));
-  BTK_CUDA(launch_choose_pc_cc(P->n_pccc, P->dim, P->d_pccc_pc, P->n_pc + P->n_far_list, P->d_pred,
-                               (float)std::log10(pair_tol), lo, P->degree,
-                               P->degree_rule == BTK_DEGREE_RULE_COST ? 1 : 0, P->d_pc_tcount, P->d_pair_weight,
-                               P->inv_cbar, P->inv_wbar, P->d_deg_pc, st));
+  const int cost_rule = P->degree_rule == BTK_DEGREE_RULE_COST ? 1 : 0;
+  BTK_CUDA(launch_choose_two_forms(P->n_pccc, P->dim, P->d_pccc_idx, P->d_pccc_coef, -1, P->n_pc + P->n_far_list,
+                                   P->d_pred, (float)std::log10(pair_tol), lo, P->degree, cost_rule,
+                                   P->d_pair_weight, P->inv_cbar, P->inv_wbar, P->d_deg_pc, st));
+  BTK_CUDA(launch_choose_two_forms(P->n_cpcc, P->dim, P->d_cpcc_idx, P->d_cpcc_coef, 0,
+                                   P->n_pc + P->n_far_list + P->n_pccc, P->d_pred, (float)std::log10(pair_tol), lo,
+                                   P->degree, cost_rule, P->d_pair_weight, P->inv_cbar, P->inv_wbar, P->d_deg_pc,
+                                   st));
   BTK_CUDA(launch_choose_leaf_pairs(P->n_pc - P->n_pc_list, P->n_conv_cc, P->dim, P->n_pc_list,
-                                    P->n_pc + P->n_far_list + P->n_pccc, P->d_pred, (float)std::log10(pair_tol), lo,
+                                    P->n_pc + P->n_far_list + P->n_pccc + P->n_cpcc, P->d_pred,
+                                    (float)std::log10(pair_tol), lo,
                                     P->degree,
                                     P->degree_rule == BTK_DEGREE_RULE_COST ? 1 : 0, P->d_pc_tcount, P->d_pc_direct,
                                     P->d_pair_weight, P->inv_cbar, P->inv_wbar, P->d_deg_pc, st));

@@ -545,36 +545,38 @@ __global__ void k_choose_leaf_pairs(int n, int n_cc, int dim, int pc0, int cc0, 
   if (has_cc) deg[j] = form == 2 ? d_best : 0;
 }
 
-// PC pairs whose target leaf holds more points than the plan degree's proxies
-// (k < n): the PC form (entry pc_idx[k]) or target-leaf proxies x
-// source-cluster proxies (CC entry cc0 + k), each at its own degrees, by the
-// same rules (threshold rule with no form meeting the tolerance: PC at hi).
-// The form not taken gets degree -1 (PC entry) or 0 (CC entry).
-__global__ void k_choose_pc_cc(int n, int dim, const int* pc_idx, int cc0, const float* pred, float log10_target,
-                               int lo, int hi, int cost_rule, const int* pc_tcount, const int* weight, float inv_cbar,
-                               float inv_wbar, int* deg) {
+// Pairs with two approximate forms, k < n: the form of entry idx[k] (PC:
+// target leaf points x source proxies, coef[k] = the target leaf's points; CP:
+// target proxies x source leaf points, coef[k] = the source leaf's points),
+// costing coef (d+1)^dim, or proxies on both sides (CC entry cc0 + k),
+// (d+1)^(2 dim); each at its own degrees, by the same rules as the other
+// pairs (threshold rule with no form meeting the tolerance: the first form at
+// hi). The form not taken gets degree off_first (its entry) or 0 (CC entry).
+__global__ void k_choose_two_forms(int n, int dim, const int* idx, const int* coef, int off_first, int cc0,
+                                   const float* pred, float log10_target, int lo, int hi, int cost_rule,
+                                   const int* weight, float inv_cbar, float inv_wbar, int* deg) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
-  const int i = pc_idx[k], j = cc0 + k;
-  const float nt = (float)pc_tcount[i];
+  const int i = idx[k], j = cc0 + k;
+  const float cf = (float)coef[k];
   const float wr = (float)weight[i] * inv_wbar;
   float best = 3.4e38f;
   int form = 1, d_best = hi;
   for (int c = max(lo, kDegLo); c <= hi && c < kDegLo + kO; ++c) {
     const float m = (float)(c + 1);
     const float md = dim == 3 ? m * m * m : m * m;
-    const float p_pc = pred[(size_t)i * kO + (c - kDegLo)], p_cc = pred[(size_t)j * kO + (c - kDegLo)];
-    float j_pc, j_cc;
+    const float p_1 = pred[(size_t)i * kO + (c - kDegLo)], p_cc = pred[(size_t)j * kO + (c - kDegLo)];
+    float j_1, j_cc;
     if (cost_rule) {
-      const float e_pc = exp10f(fminf(p_pc - log10_target, 18.f)), e_cc = exp10f(fminf(p_cc - log10_target, 18.f));
-      j_pc = nt * md * inv_cbar + wr * e_pc * e_pc;
+      const float e_1 = exp10f(fminf(p_1 - log10_target, 18.f)), e_cc = exp10f(fminf(p_cc - log10_target, 18.f));
+      j_1 = cf * md * inv_cbar + wr * e_1 * e_1;
       j_cc = md * md * inv_cbar + wr * e_cc * e_cc;
     } else {
-      j_pc = p_pc <= log10_target ? nt * md : 3.4e38f;
+      j_1 = p_1 <= log10_target ? cf * md : 3.4e38f;
       j_cc = p_cc <= log10_target ? md * md : 3.4e38f;
     }
-    if (j_pc < best) {
-      best = j_pc;
+    if (j_1 < best) {
+      best = j_1;
       form = 1;
       d_best = c;
     }
@@ -584,7 +586,7 @@ __global__ void k_choose_pc_cc(int n, int dim, const int* pc_idx, int cc0, const
       d_best = c;
     }
   }
-  deg[i] = form == 1 ? d_best : -1;
+  deg[i] = form == 1 ? d_best : off_first;
   deg[j] = form == 2 ? d_best : 0;
 }
 
@@ -944,12 +946,12 @@ cudaError_t launch_choose_leaf_pairs(int n, int n_cc, int dim, int pc0, int cc0,
   return cudaGetLastError();
 }
 
-cudaError_t launch_choose_pc_cc(int n, int dim, const int* pc_idx, int cc0, const float* pred, float log10_target,
-                                int lo, int hi, int cost_rule, const int* pc_tcount, const int* weight,
-                                float inv_cbar, float inv_wbar, int* deg, cudaStream_t s) {
+cudaError_t launch_choose_two_forms(int n, int dim, const int* idx, const int* coef, int off_first, int cc0,
+                                   const float* pred, float log10_target, int lo, int hi, int cost_rule,
+                                   const int* weight, float inv_cbar, float inv_wbar, int* deg, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_choose_pc_cc<<<(n + 255) / 256, 256, 0, s>>>(n, dim, pc_idx, cc0, pred, log10_target, lo, hi, cost_rule,
-                                                 pc_tcount, weight, inv_cbar, inv_wbar, deg);
+  k_choose_two_forms<<<(n + 255) / 256, 256, 0, s>>>(n, dim, idx, coef, off_first, cc0, pred, log10_target, lo, hi,
+                                                     cost_rule, weight, inv_cbar, inv_wbar, deg);
   count_launch();
   return cudaGetLastError();
 }
