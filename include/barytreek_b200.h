@@ -350,7 +350,8 @@ typedef struct {
    * or when no degree meets the pair tolerance under the cost rule), and,
    * where the target leaf holds more points than the plan degree's proxies,
    * target-leaf proxies x source-leaf proxies as a third (the PC pairs of
-   * such target leaves get that form as their alternative too); the
+   * such target leaves, and the CP pairs of source leaves larger than that,
+   * get the proxy-to-proxy form as their alternative too); the
    * fallback and btk_plan_execute evaluate them directly, as the reference
    * does. 0: PP pairs are always direct. */
   int leaf_far_pairs;
