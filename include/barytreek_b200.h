@@ -339,21 +339,20 @@ typedef struct {
    * ignored otherwise (btk_plan_stats.cc_groups = 0). 0: pairwise, as the
    * reference. */
   int cc_operators;
-  /* BTK_DEGREE_PER_PAIR plans only (no reference counterpart): 1 lets the
-   * degree choice approximate well-separated PP pairs too. The reference
-   * evaluates every pair of leaves directly once both have at most
+  /* BTK_DEGREE_PER_PAIR plans only (no reference counterpart). 1: the
+   * learned degree choice also decides well-separated PP pairs, which the
+   * reference always evaluates directly (both leaves hold at most
    * fmm_cluster_thresh points, a cost rule made for proxies at the plan
-   * degree; at a per-pair degree d, a pair of leaves that satisfies the MAC
-   * is cheaper as target points x source proxies when the source leaf has more
-   * than (d+1)^dim points. Such pairs join the PC pairs of the degree choice,
-   * with the direct evaluation as one more option (chosen when it is cheaper
-   * or when no degree meets the pair tolerance under the cost rule), and,
-   * where the target leaf holds more points than the plan degree's proxies,
-   * target-leaf proxies x source-leaf proxies as a third (the PC pairs of
-   * such target leaves, and the CP pairs of source leaves larger than that,
-   * get the proxy-to-proxy form as their alternative too); the
-   * fallback and btk_plan_execute evaluate them directly, as the reference
-   * does. 0: PP pairs are always direct. */
+   * degree). Each such pair is evaluated directly, as target points x
+   * source-leaf proxies at a chosen degree, or, where the target leaf holds
+   * more points than the plan degree's proxies, as proxies x proxies; the PC
+   * pairs of such target leaves and the CP pairs of source leaves larger than
+   * that choose between their own form and proxies x proxies. Under the cost
+   * rule the direct form costs n_t n_s with no error; under the threshold rule
+   * it is taken when no approximation meets the pair tolerance or costs less.
+   * btk_plan_execute, btk_plan_set_degrees and the fallback evaluate the leaf
+   * pairs directly and the other pairs in their own form, as the reference.
+   * 0: PP pairs are always direct. */
   int leaf_far_pairs;
   /* The separation bound of those pairs: non-touching leaf pairs with
    * (r_t + r_s) / |c_t - c_s| < leaf_far_theta (r: half diagonals) join the
