@@ -33,14 +33,22 @@ def problem(dim, n, dist, seed):
     return datagen.uniform_box(seed, n, dim, -1.0, 1.0)
 
 
+@pytest.mark.parametrize("leaf_far", [False, True])
 @pytest.mark.parametrize("dim,kind,dist,deg,leaf", [(3, 0, "plummer", 6, 60), (3, 2, "uniform", 5, 40),
                                                      (3, 1, "mixture", 6, 50), (2, 2, "uniform", 7, 30),
-                                                     (2, 0, "uniform", 6, 40)])
-def test_random_degrees_match_oracle(dim, kind, dist, deg, leaf, oracle):
+                                                     (2, 0, "uniform", 6, 40), (3, 2, "uniform", 2, 40),
+                                                     (2, 2, "uniform", 2, 20)])
+def test_random_degrees_match_oracle(dim, kind, dist, deg, leaf, leaf_far, oracle):
+    """Set degrees: with leaf_far_pairs the plan also holds the leaf pairs and
+    the proxy-to-proxy alternatives (at degree 2 the leaves exceed the plan
+    degree's proxies, so every alternative exists); set_degrees keeps leaf pairs
+    direct and every other pair in its own form, so the oracle is the same."""
     import barytreek_b200 as btk
     pts, q = problem(dim, 3000, dist, 5)
     tc = btk.Treecode(pts, degree=deg, cluster_size=leaf, theta=0.7, eps=1e-4, kind=kind,
-                      degree_mode=btk._lib.DEGREE_PER_PAIR, degree_min=2)
+                      degree_mode=btk._lib.DEGREE_PER_PAIR, degree_min=2, leaf_far_pairs=leaf_far)
+    if leaf_far and deg == 2:
+        assert tc.stats()["leaf_far_pairs"] > 0
     rng = np.random.default_rng(7)
     pp, pc, cp, cc = tc.lists
     assert len(pc) + len(cp) + len(cc) > 0
