@@ -148,6 +148,8 @@ SIGNATURES = {
     "btk_selector_destroy": [_vp],
     "btk_selector_weights": [_vp],
     "btk_plan_pair_count": [_vp, _vp],
+    "btk_plan_leaf_pairs": [_vp, _vp, _vp, _vp],
+    "btk_plan_set_leaf_forms": [_vp, _vp, _vp],
     "btk_selector_predict": [_vp, _ci, _vp, _vp, _vp],
     "btk_plan_pair_features": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_plan_execute_learned": [_vp, _vp, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],

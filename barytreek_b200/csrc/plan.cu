@@ -662,6 +662,9 @@ struct btk_plan {
   int *d_cpcc_idx = nullptr, *d_cpcc_coef = nullptr;  // their CP entries (pair array), source leaf points
   double leaf_theta = 0.8;  // separation bound of the leaf pairs
   int64_t conv_direct_total = 0;  // their direct evaluations (all included in evals[0])
+  int64_t evals_pp_static = 0;     // PP evaluations with every leaf pair direct
+  std::vector<int> h_conv;         // the leaf pairs' PP list indices, in plan order
+  std::vector<int> h_pc_direct;    // per PC-block pair: source leaf first point, count (leaf pairs)
   int* d_pc_direct = nullptr;
   int n_src_slots = 0, n_tgt_slots = 0;
   long long total_src_slots = 0, total_tgt_slots = 0;
@@ -749,6 +752,16 @@ void recount_far_evals(btk_plan* P) {
   P->evals[1] = P->evals[2] = P->evals[3] = 0;
   for (int i = 0; i < P->n_pc; ++i)
     if (P->h_deg_pc[i] > 0) P->evals[1] += P->h_pc_tcount[i] * sz(P->h_deg_pc[i]);
+  // leaf pairs not direct leave the PP evaluations (the form taken is counted
+  // above as PC, or below as CC)
+  P->evals[0] = P->evals_pp_static;
+  const int n_conv = P->n_pc - P->n_pc_list;
+  for (int k = 0; k < n_conv; ++k) {
+    const int i = P->n_pc_list + k;
+    const int j = P->n_far_list + P->n_pccc + P->n_cpcc + k;  // CC entry (first n_conv_cc pairs)
+    const bool direct = P->h_deg_pc[i] == 0 && (k >= P->n_conv_cc || P->h_deg_far[j] == 0);
+    if (!direct) P->evals[0] -= (int64_t)P->h_pc_tcount[i] * P->h_pc_direct[2 * i + 1];
+  }
   for (int i = 0; i < P->n_cp; ++i) P->evals[2] += sz(P->h_deg_far[i]) * P->h_cp_scount[i];
   for (int i = P->n_cp; i < P->n_far; ++i)
     if (P->h_deg_far[i] > 0) P->evals[3] += sz(P->h_deg_far[i]) * sz(P->h_deg_far[i]);
@@ -962,7 +975,10 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
     pc_entry.push_back(pp_entry[i]);
   }
   BTK_TRY(A.upload(&P->d_pc_direct, pc_direct));
+  P->h_pc_direct = pc_direct;
+  P->h_conv = conv;
   P->evals[0] = W.evals[0];
+  P->evals_pp_static = W.evals[0];
   P->n_static_items = (int)W.items.size();
   P->n_static_entries = (int)W.entries.size();
   // Far pairs: CP then CC.
@@ -1875,6 +1891,36 @@ btk_status btk_plan_set_degrees(btk_plan* P, const int* deg_pc, const int* deg_c
   if (deg_pc) std::copy(deg_pc, deg_pc + P->n_pc_list, P->h_deg_pc.begin());  // leaf pairs stay direct
   if (deg_cp) std::copy(deg_cp, deg_cp + P->n_cp, P->h_deg_far.begin());
   if (deg_cc) std::copy(deg_cc, deg_cc + n_cc, P->h_deg_far.begin() + P->n_cp);
+  BTK_CUDA(cudaMemcpyAsync(P->d_deg_pc, P->h_deg_pc.data(), sizeof(int) * P->n_pc, cudaMemcpyHostToDevice, P->stream));
+  BTK_CUDA(cudaMemcpyAsync(P->d_deg_far, P->h_deg_far.data(), sizeof(int) * P->n_far, cudaMemcpyHostToDevice,
+                           P->stream));
+  BTK_CUDA(cudaStreamSynchronize(P->stream));
+  recount_far_evals(P);
+  return BTK_OK;
+}
+
+btk_status btk_plan_leaf_pairs(const btk_plan* P, int* n_pairs, int* n_with_cc, int* pp_index) {
+  BTK_CHECK(P && n_pairs && n_with_cc, BTK_ERR_INVALID_ARGUMENT, "btk_plan_leaf_pairs: null argument");
+  *n_pairs = (int)P->h_conv.size();
+  *n_with_cc = P->n_conv_cc;
+  if (pp_index) std::copy(P->h_conv.begin(), P->h_conv.end(), pp_index);
+  return BTK_OK;
+}
+
+btk_status btk_plan_set_leaf_forms(btk_plan* P, const int* form, const int* degree) {
+  BTK_CHECK(P && form && degree, BTK_ERR_INVALID_ARGUMENT, "btk_plan_set_leaf_forms: null argument");
+  BTK_CHECK(P->degree_mode == BTK_DEGREE_PER_PAIR, BTK_ERR_INVALID_ARGUMENT, "plan is not BTK_DEGREE_PER_PAIR");
+  const int n_conv = (int)P->h_conv.size();
+  for (int k = 0; k < n_conv; ++k) {
+    BTK_CHECK(form[k] >= 0 && form[k] <= 2 && (form[k] != 2 || k < P->n_conv_cc), BTK_ERR_INVALID_ARGUMENT,
+              "leaf pair form must be 0 (direct), 1 (points x proxies) or 2 (proxies x proxies, first n_with_cc)");
+    BTK_CHECK(form[k] == 0 || (degree[k] >= P->degree_min && degree[k] <= P->degree), BTK_ERR_INVALID_ARGUMENT,
+              "leaf pair degree outside [degree_min, degree]");
+  }
+  for (int k = 0; k < n_conv; ++k) {
+    P->h_deg_pc[P->n_pc_list + k] = form[k] == 1 ? degree[k] : (form[k] == 2 ? -1 : 0);
+    if (k < P->n_conv_cc) P->h_deg_far[P->n_far_list + P->n_pccc + P->n_cpcc + k] = form[k] == 2 ? degree[k] : 0;
+  }
   BTK_CUDA(cudaMemcpyAsync(P->d_deg_pc, P->h_deg_pc.data(), sizeof(int) * P->n_pc, cudaMemcpyHostToDevice, P->stream));
   BTK_CUDA(cudaMemcpyAsync(P->d_deg_far, P->h_deg_far.data(), sizeof(int) * P->n_far, cudaMemcpyHostToDevice,
                            P->stream));

@@ -369,6 +369,17 @@ enum { BTK_DEGREE_FIXED = 0, BTK_DEGREE_PER_PAIR = 1 };
  * rejected. */
 btk_status btk_plan_set_degrees(btk_plan* plan, const int* deg_pc, const int* deg_cp, const int* deg_cc);
 
+/* Leaf pairs of a plan with leaf_far_pairs (the PP pairs the learned choice
+ * may approximate): their count, how many of them (the first) also have the
+ * proxies x proxies form, and (pp_index non-NULL) their indices in the PP list,
+ * in plan order. */
+btk_status btk_plan_leaf_pairs(const btk_plan* plan, int* n_pairs, int* n_with_cc, int* pp_index);
+/* Sets the leaf pairs' forms for btk_plan_execute (host arrays in plan order):
+ * form 0 direct, 1 target points x source-leaf proxies, 2 proxies x proxies
+ * (first n_with_cc pairs only), each at degree[k] in [degree_min,
+ * interp_degree] (ignored for form 0). The other pairs keep their degrees. */
+btk_status btk_plan_set_leaf_forms(btk_plan* plan, const int* form, const int* degree);
+
 btk_status btk_plan_create(btk_plan** plan, const btk_plan_desc* desc, btk_stream_t stream);
 btk_status btk_plan_destroy(btk_plan* plan);
 

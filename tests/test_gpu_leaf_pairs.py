@@ -91,3 +91,53 @@ def test_learned_with_leaf_pairs(case):
     assert err <= 1e-6, err
     assert rep["evals_near"] < rb["evals_near"]
     assert rep["ms_total"] < rb["ms_total"], (rep["ms_total"], rb["ms_total"])
+
+
+@pytest.mark.parametrize("dim,kind,deg,leaf", [(3, 2, 5, 40), (3, 2, 2, 40), (3, 1, 2, 60), (2, 0, 2, 30),
+                                               (2, 2, 4, 30)])
+def test_leaf_forms_match_oracle(dim, kind, deg, leaf, oracle):
+    """Forms and degrees set on every leaf pair (btk_plan_set_leaf_forms):
+    direct, target points x source-leaf proxies, or proxies x proxies (the
+    pairs whose target leaf exceeds the plan degree's proxies; at degree 2 the
+    40-point leaves do). The plain FP64 solve must equal, to 1e-12, the oracle
+    fed the same pairs as PP, PC (leaf source) and CC (leaf target and
+    source) pairs at those degrees."""
+    import ctypes
+
+    import barytreek_b200 as btk
+    from barytreek_b200 import _lib, datagen
+    from test_gpu_degrees import tree_dict
+    pts, q = datagen.uniform_box(4, 3000, dim, -1.0, 1.0)
+    tc = btk.Treecode(pts, degree=deg, cluster_size=leaf, theta=0.7, eps=1e-4, kind=kind,
+                      degree_mode=_lib.DEGREE_PER_PAIR, degree_min=2, leaf_far_pairs=True)
+    L = _lib.load()
+    n, ncc = ctypes.c_int(), ctypes.c_int()
+    _lib.check(L.btk_plan_leaf_pairs(tc._plan, ctypes.byref(n), ctypes.byref(ncc), None))
+    assert n.value > 0
+    if deg == 2:
+        assert ncc.value > 0
+    idx = np.zeros(n.value, np.int32)
+    _lib.check(L.btk_plan_leaf_pairs(tc._plan, ctypes.byref(n), ctypes.byref(ncc), _lib.ptr(idx)))
+    rng = np.random.default_rng(3)
+    form = rng.integers(0, 2, n.value).astype(np.int32)
+    form[:ncc.value] = rng.integers(0, 3, ncc.value)
+    dg = rng.integers(2, deg + 1, n.value).astype(np.int32)
+    _lib.check(L.btk_plan_set_leaf_forms(tc._plan, _lib.ptr(form), _lib.ptr(dg)))
+    out = tc.solve(q).cpu().numpy()
+    pp, pc, cp, cc = tc.lists
+    keep = np.ones(len(pp), bool)
+    keep[idx[form != 0]] = False
+    t = tree_dict(tc)
+    t["pp"], t["pc"], t["cc"] = pp[keep], np.concatenate([pc, pp[idx[form == 1]]]), np.concatenate([cc, pp[idx[form == 2]]])
+    d_pc = np.concatenate([np.full(len(pc), deg), dg[form == 1]]).astype(np.int32)
+    d_cc = np.concatenate([np.full(len(cc), deg), dg[form == 2]]).astype(np.int32)
+    ref = oracle.solve_degrees(t, kind, q, d_pc, np.full(len(cp), deg, np.int32), d_cc)
+    for c in range(tc.ncomp):
+        assert rel(out[c], ref[c]) <= 1e-12, (c, rel(out[c], ref[c]))
+    # the PP count drops by the leaf pairs that left the direct form
+    pts_t, pts_s = tc.tree_t.panels["point_count"], tc.tree_t.panels["point_count"]
+    moved = pp[idx[form != 0]]
+    st = tc.stats()
+    assert st["evals_pp"] == int(sum(int(pts_t[a]) * int(pts_s[b]) for a, b in zip(pp["target_panel"][keep],
+                                                                                     pp["source_panel"][keep])))
+    assert len(moved) == int((form != 0).sum())
