@@ -21,7 +21,11 @@
 // calls ordered on one stream do not. The first call on each device looks up
 // the scratch address with cudaGetSymbolAddress, with that device current, and
 // caches it; make that first call before any stream capture begins on that
-// device. Nothing in the scratch must start at zero: the packing kernel of the
+// device. The cached address belongs to the device's current primary context:
+// after cudaDeviceReset (or any teardown of that context) the module is
+// loaded anew and its scratch may move, so a process must not call this entry
+// point on a device again once it has reset that device. Nothing in the
+// scratch must start at zero: the packing kernel of the
 // same call writes every slot the summation kernel reads.
 #include <cstdint>
 #include <mutex>

@@ -48,7 +48,7 @@ struct WorkItem {
 static_assert(sizeof(WorkItem) == 64, "WorkItem is one 64-byte record");
 constexpr int kItemProxyTargets = 1;  // outputs go to proxy target weights
 constexpr int kItemAtomic = 2;        // another item shares these targets
-constexpr int kItemAudit = 4;         // direct-sum audit: targets T4a[t_begin + i], outputs aout[c][t_begin + i]
+constexpr int kItemAudit = 4;         // FP64 direct-sum audit: targets T4a[t_begin + i], outputs aout[c][t_begin + i]
 
 struct Entry {
   int s_begin;  // first source in the S4 array
@@ -74,7 +74,18 @@ struct InteractParams {
   double scale[4];
   int* ticket;
   int* status;
+  // Polls of a chunk's mbarrier before the block gives up (sets *status to
+  // BTK_ERR_DEVICE_TIMEOUT and leaves); 0 gives up at the first wait (tests
+  // of the error path). In-flight copies are always drained with kDrainLimit.
+  uint32_t wait_limit;
+  // The last n_audit_items items (kItemAudit) are handed out at every
+  // audit_every-th ticket instead of after the others (0: in array order), so
+  // the FP64 audit items share the SMs with the FP32 work of the solve.
+  int n_audit_items;
+  int audit_every;
 };
+constexpr uint32_t kWaitLimitDefault = 1u << 22;
+constexpr uint32_t kDrainLimit = 1u << 22;
 
 constexpr int kInteractThreads = 128;
 constexpr int kTargetsPerThread = 2;

@@ -27,7 +27,17 @@ namespace {
 
 constexpr int kChunk = 256;     // sources per shared-memory chunk (8 KB of double4)
 constexpr int kStages = 3;      // ring depth
-constexpr uint32_t kWaitLimit = 1u << 22;  // polls of try_wait before giving up
+
+// Work item of a ticket. With p.audit_every = k > 0 the n_audit_items audit
+// items (stored last) take tickets k-1, 2k-1, ...; the other items keep their
+// order in the remaining tickets (a bijection onto [0, n_items) while
+// n_audit_items * k <= n_items).
+__device__ __forceinline__ int item_of_ticket(const InteractParams& p, int t) {
+  const int k = p.audit_every, na = p.n_audit_items;
+  if (k <= 0 || na <= 0) return t;
+  if ((t + 1) % k == 0 && (t + 1) / k <= na) return p.n_items - na + (t + 1) / k - 1;
+  return t - min(na, t / k);
+}
 
 template <int DIM, int KIND>
 struct KernelTraits {
@@ -107,7 +117,7 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
     __syncthreads();
     const int it = s_item;
     if (it >= p.n_items || s_abort) break;
-    const WorkItem w = p.items[it];
+    const WorkItem w = p.items[item_of_ticket(p, it)];
     if (w.t_count <= 0 || w.s_total <= 0) continue;  // unused tile of a per-pair-degree item block
     const int n_chunks = (w.s_total + kChunk - 1) / kChunk;
 
@@ -154,7 +164,7 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
     for (int c = 0; c < n_chunks; ++c) {
       const int stage = (g + c) % kStages;
       const uint32_t parity = ((g + c) / kStages) & 1u;
-      if (!mbar_wait_bounded(&bars[stage], parity, kWaitLimit)) {
+      if (!mbar_wait_bounded(&bars[stage], parity, p.wait_limit)) {
         s_abort = 1;
         s_fail_chunk = g + c;
         atomicCAS(p.status, 0, (int)BTK_ERR_DEVICE_TIMEOUT);
@@ -203,7 +213,7 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
   // flight before the block's shared memory is released.
   if (s_abort && tid == 0) {
     for (uint32_t k = s_fail_chunk; k < issued; ++k)
-      mbar_wait_bounded(&bars[k % kStages], (k / kStages) & 1u, kWaitLimit);
+      mbar_wait_bounded(&bars[k % kStages], (k / kStages) & 1u, kDrainLimit);
   }
 }
 
@@ -354,7 +364,7 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
     __syncthreads();
     const int it = s_item;
     if (it >= p.n_items || s_abort) break;
-    const WorkItem w = p.items[it];
+    const WorkItem w = p.items[item_of_ticket(p, it)];
     if (w.t_count <= 0 || w.s_total <= 0) continue;  // unused tile of a per-pair-degree item block
     const int n_chunks = (w.s_total + kChunk - 1) / kChunk;
     const float thr = fmaxf(w.hx, fmaxf(w.hy, w.hz));  // near sources at least this far from the box: FP32 path
@@ -387,12 +397,68 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
     // 32-target halves in use (warp-uniform), so a partly filled tile leaves
     // its idle warps' issue slots to other blocks.
     const int nu = w.t_count > tbase + 32 ? 2 : (w.t_count > tbase ? 1 : 0);
+
+    if (w.flags & kItemAudit) {
+      // The audit's direct sum, in FP64 like the reference's
+      // (src/direct_sum_impl.hpp:34-94): absolute coordinates, the FP64
+      // reciprocal square root, FP64 sums. Sources are read from the FP64
+      // stage itself, so a stage is refilled only after the next chunk's
+      // barrier (every thread has finished it): chunk c - 1 + kStages is
+      // issued at chunk c, one barrier per chunk.
+      double ax[TPT], ay[TPT], az[TPT], a64[TPT][NC];
+#pragma unroll
+      for (int u = 0; u < TPT; ++u) {
+        const double4 t = p.T4a[w.t_begin + min(tbase + u * 32 + lane, w.t_count - 1)];
+        ax[u] = t.x;
+        ay[u] = t.y;
+        az[u] = t.z;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) a64[u][c] = 0.0;
+      }
+      for (int c = 0; c < n_chunks; ++c) {
+        const int stage = (g + c) % kStages;
+        const uint32_t parity = ((g + c) / kStages) & 1u;
+        if (!mbar_wait_bounded(&bars[stage], parity, p.wait_limit)) {
+          s_abort = 1;
+          s_fail_chunk = g + c;
+          atomicCAS(p.status, 0, (int)BTK_ERR_DEVICE_TIMEOUT);
+        }
+        __syncthreads();
+        if (s_abort) break;
+        if (tid == 0 && c >= 1 && c - 1 + kStages < n_chunks) issue(c - 1 + kStages);
+        const int cnt = min(kChunk, w.s_total - c * kChunk);
+        const double4* sb = sbuf[stage];
+        if (nu == 2) {
+#pragma unroll 2
+          for (int j = 0; j < cnt; ++j) {
+            const double4 sj = sb[j];
+            eval_fp64<DIM, KIND, true>(ax[0], ay[0], az[0], sj, p.eps2, a64[0]);
+            eval_fp64<DIM, KIND, true>(ax[1], ay[1], az[1], sj, p.eps2, a64[1]);
+          }
+        } else if (nu == 1) {
+#pragma unroll 2
+          for (int j = 0; j < cnt; ++j) eval_fp64<DIM, KIND, true>(ax[0], ay[0], az[0], sb[j], p.eps2, a64[0]);
+        }
+      }
+      if (s_abort) break;
+      g += n_chunks;
+#pragma unroll
+      for (int u = 0; u < TPT; ++u) {
+        const int i = tbase + u * 32 + lane;
+        if (i < w.t_count) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) atomicAdd(p.aout[c] + w.t_begin + i, a64[u][c] * p.scale[c]);
+        }
+      }
+      continue;
+    }
+
     TargetPair T[TPT];
     double acc[TPT][NC], comp[TPT][NC];
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
       const int i = min(tbase + u * 32 + lane, w.t_count - 1);
-      const double4 t = ((w.flags & kItemAudit) ? p.T4a : p.T4)[w.t_begin + i];
+      const double4 t = p.T4[w.t_begin + i];
       float h, l;
       split_rel(t.x, w.cx, h, l);
       T[u].x = make_float2(h, h);
@@ -410,7 +476,7 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
     for (int c = 0; c < n_chunks; ++c) {
       const int stage = (g + c) % kStages;
       const uint32_t parity = ((g + c) / kStages) & 1u;
-      if (!mbar_wait_bounded(&bars[stage], parity, kWaitLimit)) {
+      if (!mbar_wait_bounded(&bars[stage], parity, p.wait_limit)) {
         s_abort = 1;
         s_fail_chunk = g + c;
         atomicCAS(p.status, 0, (int)BTK_ERR_DEVICE_TIMEOUT);
@@ -550,11 +616,10 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
     for (int u = 0; u < TPT; ++u) {
       const int i = tbase + u * 32 + lane;
       if (i < w.t_count) {
-        const bool audit = (w.flags & kItemAudit) != 0;
-        const int idx = audit ? w.t_begin + i : p.T_out[w.t_begin + i];
+        const int idx = p.T_out[w.t_begin + i];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          double* dst = (audit ? p.aout[c] : (w.flags & kItemProxyTargets) ? p.ptw[c] : p.out[c]) + idx;
+          double* dst = ((w.flags & kItemProxyTargets) ? p.ptw[c] : p.out[c]) + idx;
           const double v = (acc[u][c] + comp[u][c]) * p.scale[c];
           if (w.flags & kItemAtomic)
             atomicAdd(dst, v);
@@ -566,7 +631,7 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
   }
   if (s_abort && tid == 0) {
     for (uint32_t k = s_fail_chunk; k < issued; ++k)
-      mbar_wait_bounded(&bars[k % kStages], (k / kStages) & 1u, kWaitLimit);
+      mbar_wait_bounded(&bars[k % kStages], (k / kStages) & 1u, kDrainLimit);
   }
 }
 

@@ -4,6 +4,7 @@
 #include <array>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -553,6 +554,9 @@ struct InteractCtx {
   int* d_ticket_status = nullptr;  // [0] ticket, [1] status
   const double4* d_T4a = nullptr;  // audit targets and outputs (kItemAudit items)
   Ptr4 aout{};
+  int n_audit_items = 0;  // the last n_audit_items of the n_items are audit items
+  int audit_every = 0;    // ... handed out at every audit_every-th ticket (0: last)
+  uint32_t wait_limit = kWaitLimitDefault;
 };
 
 btk_status run_interactions(const InteractCtx& C, const double4* S4, const double4* T4, const int* T_out,
@@ -575,6 +579,9 @@ btk_status run_interactions(const InteractCtx& C, const double4* S4, const doubl
   kind_scales(C.dim, C.kind, p.scale);
   p.ticket = C.d_ticket_status;
   p.status = C.d_ticket_status + 1;
+  p.wait_limit = C.wait_limit;
+  p.n_audit_items = C.n_audit_items;
+  p.audit_every = C.audit_every;
   const bool guard = p.eps2 < 1.1754943508222875e-38;
   int per_sm = interact_blocks_per_sm(C.dim, C.kind, C.precision, guard);
   if (per_sm <= 0) per_sm = 1;
@@ -680,6 +687,7 @@ struct btk_plan {
   int *d_far_type = nullptr, *d_far_tgt = nullptr, *d_far_src = nullptr;
   double* d_tgt_centre = nullptr;
   int *d_deg_pc = nullptr, *d_deg_far = nullptr;  // the degrees in force
+  bool deg_learned = false;  // d_deg_* hold a learned solve's choice, not h_deg_*
   double* d_ptwm = nullptr;                       // ncomp x total_tgt_slots
   // host copies for work accounting
   std::vector<int> h_pc_tcount, h_cp_scount, h_deg_pc, h_deg_far;
@@ -1370,6 +1378,14 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
   Side& T = P->tgt;
   Side& S = *P->src;
   const int Pt = T.h.panel_count;
+  if (P->deg_learned) {
+    // A learned solve left its own degrees and forms on the device: this
+    // solve uses the ones set by btk_plan_set_degrees / btk_plan_set_leaf_forms.
+    BTK_CUDA(cudaMemcpyAsync(P->d_deg_pc, P->h_deg_pc.data(), sizeof(int) * P->n_pc, cudaMemcpyHostToDevice, st));
+    BTK_CUDA(cudaMemcpyAsync(P->d_deg_far, P->h_deg_far.data(), sizeof(int) * P->n_far, cudaMemcpyHostToDevice, st));
+    P->deg_learned = false;
+  }
+  BTK_CUDA(cudaMemsetAsync(P->d_ticket_status + 1, 0, sizeof(int), st));  // this solve's device status
   BTK_CUDA(cudaEventRecord(P->ev[0], st));
   // Upward.
   BTK_CUDA(launch_gather(S.n_points, S.d_perm, xs, ys, P->dim == 3 ? zs : nullptr, charges, P->d_S4, st));
@@ -1441,20 +1457,15 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
 namespace {
 
 // The audit: a fixed, seeded 1% sample of the targets (at least one when
-// there are targets) and work items for the FP64-accurate direct sum over every
-// source, built on the host at plan creation. The sampled targets are sorted
-// along the leaf order (a space-filling order of the tree) and cut into tiles
-// of kTile, so a tile covers a compact region; each tile lists the source
-// leaves near its box first (hi/lo coordinate path, as touching PP sources)
-// and the rest after (plain FP32 path, separation at least half the box's
-// side), relative to the box centre, in pieces of about kAuditPiece sources so
-// the items are small tail-fillers of the solve's launch.
+// there are targets), spread evenly over the index range, and work items for
+// its FP64 direct sum over every source, built on the host at plan creation:
+// tiles of kTile sampled targets x pieces of kAuditPiece consecutive sources
+// of the leaf-ordered source array (kItemAudit | kItemAtomic; the interaction
+// kernels evaluate them in FP64 whatever the plan's precision).
 constexpr int kAuditPiece = 4096;
 
 void build_audit_work(const btk_plan* P, int entry_base, AuditWork& W) {
-  const Side& T = P->tgt;
-  const Side& S = *P->src;
-  const int nt = T.n_points;
+  const int nt = P->tgt.n_points, ns = P->src->n_points;
   const int na = nt > 0 ? std::max(1, nt / 100) : 0;
   W.orig.assign(na, 0);
   // Evenly spread, seeded offsets (SplitMix64-style hash) over the index range.
@@ -1466,82 +1477,18 @@ void build_audit_work(const btk_plan* P, int entry_base, AuditWork& W) {
     const int64_t lo = (int64_t)k * nt / na, hi = (int64_t)(k + 1) * nt / na;
     W.orig[k] = (int)(lo + (int64_t)(z % (uint64_t)std::max<int64_t>(1, hi - lo)));
   }
-  // Leaf-order position and leaf of every target (when the host knows the order).
-  std::vector<int> pos_of, leaf_at;
-  const bool spatial = (int)T.h_perm.size() == nt && nt > 0;
-  if (spatial) {
-    pos_of.assign(nt, 0);
-    for (int p = 0; p < nt; ++p) pos_of[T.h_perm[p]] = p;
-    leaf_at.assign(nt, -1);
-    for (int L : T.leaves)
-      for (int j = 0; j < T.h.point_count[L]; ++j) leaf_at[T.leaf_begin[L] + j] = L;
-    std::sort(W.orig.begin(), W.orig.end(), [&](int a, int b) { return pos_of[a] < pos_of[b]; });
-  }
-  const int dim = T.h.dim;
-  for (int t0 = 0; t0 < na; t0 += kTile) {
-    const int tc = std::min(kTile, na - t0);
-    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    if (spatial) {
-      for (int d = 0; d < dim; ++d) {
-        lo[d] = 1e300;
-        hi[d] = -1e300;
-      }
-      for (int k = t0; k < t0 + tc; ++k) {
-        const PanelGeom& g = T.h.geom[leaf_at[pos_of[W.orig[k]]]];
-        for (int d = 0; d < dim; ++d) {
-          lo[d] = std::min(lo[d], g.lo[d]);
-          hi[d] = std::max(hi[d], g.hi[d]);
-        }
-      }
-    } else {
-      for (int d = 0; d < dim; ++d) {
-        lo[d] = S.h.geom[0].lo[d];
-        hi[d] = S.h.geom[0].hi[d];
-      }
-    }
-    double c[3] = {0, 0, 0}, side = 0;
-    for (int d = 0; d < dim; ++d) {
-      c[d] = 0.5 * (lo[d] + hi[d]);
-      side = std::max(side, hi[d] - lo[d]);
-    }
-    // Source leaves: near the tile's box first, then the rest.
-    std::vector<Entry> near, far;
-    for (int L : S.leaves) {
-      const PanelGeom& g = S.h.geom[L];
-      double gap = 0;
-      for (int d = 0; d < dim; ++d) gap = std::max(gap, std::max(g.lo[d] - hi[d], lo[d] - g.hi[d]));
-      (spatial && gap > 0.5 * side ? far : near).push_back(Entry{S.leaf_begin[L], S.h.point_count[L]});
-    }
-    int n_near = 0;
-    for (const Entry& e : near) n_near += e.s_count;
-    const int e_first = (int)W.entries.size();
-    W.entries.insert(W.entries.end(), near.begin(), near.end());
-    W.entries.insert(W.entries.end(), far.begin(), far.end());
-    const int e_last = (int)W.entries.size();
-    int k = e_first, before = 0;  // sources of this tile's list ahead of entry k
-    while (k < e_last) {
-      const int kb = k;
-      int st = 0;
-      while (k < e_last && (st == 0 || st + W.entries[k].s_count <= kAuditPiece)) st += W.entries[k++].s_count;
+  for (int s0 = 0; s0 < ns; s0 += kAuditPiece) W.entries.push_back(Entry{s0, std::min(kAuditPiece, ns - s0)});
+  for (int t0 = 0; t0 < na; t0 += kTile)
+    for (int e = 0; e < (int)W.entries.size(); ++e) {
       WorkItem w{};
       w.t_begin = t0;
-      w.t_count = tc;
-      w.e_begin = entry_base + kb;
-      w.e_end = entry_base + k;
-      w.s_total = st;
+      w.t_count = std::min(kTile, na - t0);
+      w.e_begin = entry_base + e;
+      w.e_end = entry_base + e + 1;
+      w.s_total = W.entries[e].s_count;
       w.flags = kItemAtomic | kItemAudit;
-      w.near_total = std::max(0, std::min(st, n_near - before));
-      w.cx = c[0];
-      w.cy = c[1];
-      w.cz = c[2];
-      // unsorted sample (no tile box): every near source keeps the hi/lo path
-      w.hx = spatial ? (float)(0.5 * (hi[0] - lo[0])) : 3.0e38f;
-      w.hy = spatial ? (float)(0.5 * (hi[1] - lo[1])) : 3.0e38f;
-      w.hz = spatial && dim == 3 ? (float)(0.5 * (hi[2] - lo[2])) : (spatial ? 0.f : 3.0e38f);
       W.items.push_back(w);
-      before += st;
     }
-  }
 }
 
 // Uploads the audit sample and its work items into ictx's arrays at
@@ -1651,7 +1598,9 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   const int Pt = T.h.panel_count;
   cudaEvent_t e[4];
   for (auto& x : e) BTK_CUDA(cudaEventCreate(&x));
+  BTK_CUDA(cudaMemsetAsync(P->d_ticket_status + 1, 0, sizeof(int), st));  // this solve's device status
   BTK_CUDA(cudaEventRecord(e[0], st));
+  P->deg_learned = true;
   // Upward pass and features, then the selector's degrees.
   BTK_TRY(btk_plan_pair_features(P, xs, ys, zs, charges, P->d_feat, stream));
   BTK_CUDA(launch_mlp_infer(P->n_pairs, sel->d_w, sel->norm, P->d_feat, P->d_pred, st));
@@ -1721,13 +1670,19 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     BTK_TRY(run_downward(T, P->ncomp, P->d_T4, w, o, st));
     return BTK_OK;
   };
-  // The audit (direct sum at the sampled targets) runs as the last work items
-  // of the solve's own launch, filling its tail.
+  // The audit (FP64 direct sum at the sampled targets) runs as work items of
+  // the solve's own launch.
   BTK_CUDA(launch_gather(P->n_audit, P->d_audit_orig, xt, yt, P->dim == 3 ? zt : nullptr, nullptr, P->d_audit_T4, st));
   BTK_CUDA(cudaMemsetAsync(P->d_audit_out, 0, sizeof(double) * (size_t)P->ncomp * std::max(P->n_audit, 1), st));
   BTK_CUDA(cudaMemsetAsync(P->d_audit_sums, 0, 2 * sizeof(double), st));
   InteractCtx with_audit = P->ictx;
   with_audit.n_items = P->n_items_main + P->n_audit_items;
+  with_audit.n_audit_items = P->n_audit_items;
+  {
+    const char* sp = getenv("BTK_AUDIT_SPREAD");
+    if (sp && atoi(sp) > 0 && P->n_audit_items > 0)
+      with_audit.audit_every = with_audit.n_items / P->n_audit_items;
+  }
   with_audit.d_T4a = P->d_audit_T4;
   for (int c = 0; c < P->ncomp; ++c) with_audit.aout.p[c] = P->d_audit_out + (size_t)c * P->n_audit;
   BTK_TRY(solve(with_audit));
@@ -1895,6 +1850,7 @@ btk_status btk_plan_set_degrees(btk_plan* P, const int* deg_pc, const int* deg_c
   BTK_CUDA(cudaMemcpyAsync(P->d_deg_far, P->h_deg_far.data(), sizeof(int) * P->n_far, cudaMemcpyHostToDevice,
                            P->stream));
   BTK_CUDA(cudaStreamSynchronize(P->stream));
+  P->deg_learned = false;
   recount_far_evals(P);
   return BTK_OK;
 }
@@ -1925,7 +1881,22 @@ btk_status btk_plan_set_leaf_forms(btk_plan* P, const int* form, const int* degr
   BTK_CUDA(cudaMemcpyAsync(P->d_deg_far, P->h_deg_far.data(), sizeof(int) * P->n_far, cudaMemcpyHostToDevice,
                            P->stream));
   BTK_CUDA(cudaStreamSynchronize(P->stream));
+  P->deg_learned = false;
   recount_far_evals(P);
+  return BTK_OK;
+}
+
+btk_status btk_plan_set_wait_limit(btk_plan* P, long long polls) {
+  BTK_CHECK(P, BTK_ERR_INVALID_ARGUMENT, "null plan");
+  P->ictx.wait_limit = polls < 0 ? kWaitLimitDefault : (uint32_t)std::min<long long>(polls, 0xffffffffLL);
+  return BTK_OK;
+}
+
+btk_status btk_plan_audit_targets(const btk_plan* P, int* n, int* orig) {
+  BTK_CHECK(P && n, BTK_ERR_INVALID_ARGUMENT, "btk_plan_audit_targets: null argument");
+  *n = P->n_audit;
+  if (orig && P->n_audit > 0)
+    BTK_CUDA(cudaMemcpy(orig, P->d_audit_orig, sizeof(int) * P->n_audit, cudaMemcpyDeviceToHost));
   return BTK_OK;
 }
 

@@ -331,7 +331,7 @@ class Treecode:
         return out
 
     def solve_learned(self, charges, selector, tol=1e-6, pair_tol=None, degree_lo=4, out=None):
-        """Learned-degree solve with a 1% direct-sum audit and fallback
+        """Learned-degree solve with a 1% FP64 direct-sum audit and fallback
         (btk_plan_execute_learned). Returns (out tensor, report dict)."""
         import torch
 
@@ -351,6 +351,20 @@ class Treecode:
         r = {k: getattr(rep, k) for k, _ in rep._fields_ if k != "degree_hist"}
         r["degree_hist"] = list(rep.degree_hist)
         return out, r
+
+    def set_wait_limit(self, polls: int):
+        """Polls of each chunk barrier before the interaction kernel gives up
+        (btk_plan_set_wait_limit); 0 gives up at once, < 0 restores the default."""
+        check(load().btk_plan_set_wait_limit(self._plan, int(polls)))
+
+    def audit_targets(self) -> np.ndarray:
+        """Original indices of the targets the learned solve's audit checks."""
+        n = ctypes.c_int(0)
+        check(load().btk_plan_audit_targets(self._plan, ctypes.byref(n), None))
+        out = np.zeros(n.value, np.int32)
+        if n.value:
+            check(load().btk_plan_audit_targets(self._plan, ctypes.byref(n), ptr(out)))
+        return out
 
     def last_timing(self) -> dict:
         ms = (ctypes.c_float * 5)()

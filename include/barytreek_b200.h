@@ -275,7 +275,8 @@ btk_status btk_direct_sum(int dim, int kind, double eps, int nt, const double* x
  * device). One scratch per device: overlapping calls on one device (threads,
  * or streams not ordered against each other) race. The first call on a
  * device looks up the scratch address (cudaGetSymbolAddress); make it before
- * any stream capture begins on that device. */
+ * any stream capture begins on that device. The address is kept for the
+ * process: do not call this again on a device after cudaDeviceReset there. */
 btk_status btk_direct_sum_noalloc(int dim, int kind, double eps, int nt, const double* xt, const double* yt,
                                   const double* zt, int ns, const double* xs, const double* ys, const double* zs,
                                   const double* charges, double* out, btk_stream_t stream);
@@ -350,8 +351,11 @@ typedef struct {
    * that choose between their own form and proxies x proxies. Under the cost
    * rule the direct form costs n_t n_s with no error; under the threshold rule
    * it is taken when no approximation meets the pair tolerance or costs less.
-   * btk_plan_execute, btk_plan_set_degrees and the fallback evaluate the leaf
-   * pairs directly and the other pairs in their own form, as the reference.
+   * Leaf pairs are direct until btk_plan_set_leaf_forms sets their forms;
+   * btk_plan_set_degrees leaves those forms as they are. btk_plan_execute
+   * uses the degrees and forms set by those two calls (a learned solve does
+   * not change them), and the learned solve's fallback evaluates every leaf
+   * pair directly and the other pairs at the plan degree, as the reference.
    * 0: PP pairs are always direct. */
   int leaf_far_pairs;
   /* The separation bound of those pairs: non-touching leaf pairs with
@@ -423,6 +427,20 @@ btk_status btk_plan_execute(btk_plan* plan, const double* xt, const double* yt, 
  * [2] downward, [3] total, [4] the interaction kernel alone. */
 btk_status btk_plan_last_timing(btk_plan* plan, float* ms);
 
+/* Polls of each shared-memory chunk's mbarrier the interaction kernels make
+ * before giving up (no reference counterpart). A block that gives up waits
+ * for its copies still in flight, stops taking work and sets the plan's
+ * device status, which the next btk_plan_last_timing (or the learned solve
+ * itself) returns as BTK_ERR_DEVICE_TIMEOUT; the solve's results are then
+ * incomplete. 0 gives up at the first wait (to exercise that path);
+ * polls < 0 restores the default (2^22). Each solve clears the status. */
+btk_status btk_plan_set_wait_limit(btk_plan* plan, long long polls);
+
+/* The targets the learned solve's audit checks (a fixed, seeded 1% of the
+ * targets, at least one): their count, and (orig non-NULL, host) their
+ * original indices in the order the audit evaluates them. */
+btk_status btk_plan_audit_targets(const btk_plan* plan, int* n, int* orig);
+
 /* One call from host buffers: builds the tree and lists with the host tree
  * functions, creates a plan, copies inputs to the device, solves, copies
  * out[ncomp][n] back (host) and destroys the plan. Sources = targets. */
@@ -461,7 +479,7 @@ btk_status btk_plan_pair_features(btk_plan* plan, const double* xs, const double
                                   const double* charges, float* features, btk_stream_t stream);
 
 typedef struct {
-  double audit_rel_l2; /* treecode vs direct sum over the audited targets */
+  double audit_rel_l2; /* treecode vs FP64 direct sum over the audited targets */
   int audit_targets;   /* 1% of the targets (fixed, seeded sample) */
   int fell_back;       /* 1: audit above tol, the fixed-degree FP64 result was returned */
   int64_t evals_near;  /* PP evaluations (approximated leaf pairs excluded) */
@@ -477,7 +495,9 @@ typedef struct {
 /* Learned-degree solve: upward pass, features, network, per-pair degree =
  * the smallest d in [max(degree_lo, degree_min), interp_degree] whose
  * predicted error is <= pair_tol, interactions at those degrees (the plan's
- * precision), downward pass; then a direct-sum audit of 1% of the targets.
+ * precision), downward pass; then an FP64 direct-sum audit of 1% of the
+ * targets (btk_plan_audit_targets), evaluated as FP64 work items of the
+ * solve's own interaction launch whatever the plan's precision.
  * When the audit's relative L2 exceeds tol, the fixed-degree FP64 result is
  * computed and returned instead (report->fell_back = 1). Synchronises the
  * stream once (to read the audit). out as btk_plan_execute.
@@ -528,12 +548,11 @@ btk_status btk_mlp_gradient(const void* w_bf16, int n, const float* xn, const fl
 btk_status btk_mlp_adam(float* master, void* w_bf16, const float* grad, float* m, float* v, int step, float lr,
                         btk_stream_t stream);
 
-/* Sustained fused-multiply-add rate of this GPU's FP64 (which = 0) or FP32
- * (which = 1: scalar FFMA; which = 2: packed f32x2 FFMA2) CUDA-core pipe, in
- * TFLOP/s (2 flops per FMA), measured by a probe kernel with independent FMA
- * chains on every SM; which = 3 gives the MUFU reciprocal-square-root rate in
- * T results/s. The roofline denominators for the pairwise interaction
- * kernels. */
+/* Benchmark infrastructure (no reference counterpart): the sustained
+ * fused-multiply-add rate of this GPU's FP64 (which = 0) or FP32 (which = 1)
+ * CUDA-core pipe in TFLOP/s (2 flops per FMA), measured by a probe kernel with
+ * independent FMA chains on every SM; the measured roofline denominator of
+ * the pairwise interaction kernels. */
 btk_status btk_measure_pipe_peak(int which, double* tflops, btk_stream_t stream);
 
 /* ---- 5. Batches of independent problems ---------------------------------

@@ -189,6 +189,7 @@ class RefLib:
         L.btkref_solve.argtypes = [vp, ci, ci, vp, vp, vp, vp, vp]
         L.btkref_direct.argtypes = [ci, ci, ci, vp, vp, vp, ci, vp, vp, vp, vp, cd, vp]
         L.btkref_time_sample_3d.argtypes = [vp, ci, ci, vp, vp, vp, vp]
+        L.btkref_solve_leaves.argtypes = [vp, ci, vp, ci, vp, vp]
         L.btkref_read_namelist.argtypes = [ctypes.c_char_p, ci, vp]
         L.btkref_set_threads.argtypes = [ci]
         self.set_threads(threads)
@@ -284,6 +285,26 @@ class RefTree:
         if rc:
             raise RuntimeError(f"btkref_solve rc={rc}")
         return {"psw": psw, "ptw_mid": ptw, "mid": mid, "out": out}
+
+    def solve_leaves(self, kind, q, leaves):
+        """The fixed solve at the targets of the given leaf panels only (upward
+        pass in full, interaction pairs whose target is one of those leaves or
+        an ancestor, downward pass along those panels). Returns (ncomp, nt);
+        only the sampled leaves' targets hold the full solution."""
+        nt = len(self.targets[0])
+        nc = 3 if kind == VEL else 1
+        leaves = np.ascontiguousarray(leaves, dtype=np.int32)
+        out = np.zeros((nc, nt))
+        rc = self.ref.lib.btkref_solve_leaves(self.h, kind, _p(_f64(q)), len(leaves), _p(leaves), _p(out))
+        if rc:
+            raise RuntimeError(f"btkref_solve_leaves rc={rc}")
+        return out
+
+    def leaf_targets(self, leaves):
+        """Original indices of the targets in the given leaf panels."""
+        t = self.trees[0]
+        cnt = t["panels"]["point_count"]
+        return np.concatenate([t["inside"][L, :cnt[L]] for L in leaves]).astype(np.int64)
 
     def time_sample_3d(self, kind, stride, q):
         sec, scale, ev = np.zeros(8), np.zeros(8), np.zeros(2)

@@ -7,7 +7,7 @@
 // examples/example_poisson_vel_3d.cpp, examples/example_poisson_2d_split.cpp):
 // build the tree and interaction lists, run the upward pass, the interaction
 // phase and the downward pass, and the direct sum, all through the reference's
-// own functions and functors. It adds three things the examples do not have:
+// own functions and functors. It adds four things the examples do not have:
 //
 //  * explicit inputs (seeded points instead of std::random_device) and access
 //    to every intermediate array, so that tests can compare phase by phase;
@@ -19,7 +19,10 @@
 //    fixed variant calls the reference's own functors
 //    (src/downward_pass_impl.hpp:109-237, :239-379) on non-leaf parents only and
 //    on every leaf. Nothing under the reference tree is edited;
-//  * strided, timed samples of each phase for the CPU baseline.
+//  * strided, timed samples of each phase for the CPU baseline;
+//  * a solve restricted to the targets of sampled leaves (full upward pass,
+//    the pairs of those leaves and their ancestors, the downward pass along
+//    them) for parity checks at full workload sizes.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -344,6 +347,116 @@ int btkref_solve(void* p, int kind, int fixed, const double* charges, double* ps
   return 0;
 }
 
+// The same solve restricted to the targets of a few sampled leaves, for
+// parity checks at sizes where a whole reference solve takes too long. The
+// upward pass runs in full (the reference's upward_pass_2d/3d). Then:
+//   * needed target panels = the sampled leaves and all their ancestors;
+//   * each interaction list keeps the pairs whose target panel is needed, in
+//     list order, and the reference's own poisson_fmm_interactions_* /
+//     poisson_vel_fmm_interactions_3d runs on those sub-lists (the counts in a
+//     copy of the RunConfig are set to the sub-list lengths);
+//   * the fixed downward pass runs parent_to_child on (non-leaf parent, child)
+//     pairs whose child is needed, level by level, and leaf_to_point on the
+//     sampled leaves only.
+// Every needed panel then holds exactly what the full solve gives it, so the
+// output at the sampled leaves' targets equals the full (fixed) solve's. Other
+// targets hold partial sums; callers read the sampled leaves' targets only.
+// kind 0 potential, 1 3-D velocity; out [ncomp x nt].
+int btkref_solve_leaves(void* p, int kind, const double* charges, int n_leaves, const int* leaves, double* out) {
+  Handle& h = *static_cast<Handle*>(p);
+  RunConfig c = h.cfg;
+  Tree& T = h.tgt;
+  Tree& S = h.source();
+  if (kind == 1 && c.dim != 3) return 2;
+  const int Pt = T.info.panel_count;
+  std::vector<char> needed(Pt, 0), sampled(Pt, 0);
+  for (int k = 0; k < n_leaves; ++k) {
+    int i = leaves[k];
+    if (i < 0 || i >= Pt || !is_leaf_panel(h, T, i)) return 3;
+    sampled[i] = 1;
+    while (i >= 0 && !needed[i]) {
+      needed[i] = 1;
+      i = c.dim == 2 ? T.hp2(i).parent_id : T.hp3(i).parent_id;
+    }
+  }
+  auto filter = [&](const view_interact_host& L, const char* label, int& count) {
+    std::vector<interact_pair> keep;
+    for (int i = 0; i < (int)L.extent(0); ++i)
+      if (needed[L(i).target_panel]) keep.push_back(L(i));
+    count = (int)keep.size();
+    view_interact d(label, std::max<size_t>(keep.size(), 1));
+    if (!keep.empty()) std::memcpy(d.data(), keep.data(), sizeof(interact_pair) * keep.size());
+    return d;
+  };
+  view_interact fpp = filter(h.pp, "pp", c.fmm_pp_count), fpc = filter(h.pc, "pc", c.fmm_pc_count);
+  view_interact fcp = filter(h.cp, "cp", c.fmm_cp_count), fcc = filter(h.cc, "cc", c.fmm_cc_count);
+  c.fmm_interaction_count = c.fmm_pp_count + c.fmm_pc_count + c.fmm_cp_count + c.fmm_cc_count;
+
+  const int ipc = c.interp_point_count;
+  const int ncomp = kind == 1 ? 3 : 1;
+  view_real q = make_view("charges", S.n, charges);
+  view_reall w_src("psw", S.info.panel_count, ipc);
+  std::vector<view_reall> w_tgt;
+  std::vector<view_real> sol;
+  for (int k = 0; k < ncomp; ++k) {
+    w_tgt.emplace_back("ptw", Pt, ipc);
+    sol.emplace_back("sol", T.n);
+  }
+  if (c.dim == 2)
+    upward_pass_2d(c, S.info, S.x, S.y, q, S.p2, w_src, S.leaf_of);
+  else
+    upward_pass_3d(c, S.info, S.x, S.y, S.z, q, S.p3, w_src, S.leaf_of);
+  if (c.dim == 2)
+    poisson_fmm_interactions_2d(c, T.x, T.y, S.x, S.y, q, sol[0], S.inside, T.inside, w_src, w_tgt[0], fpp, fpc, fcp,
+                                fcc, S.p2, T.p2);
+  else if (kind == 0)
+    poisson_fmm_interactions_3d(c, T.x, T.y, T.z, S.x, S.y, S.z, q, sol[0], S.inside, T.inside, w_src, w_tgt[0], fpp,
+                                fpc, fcp, fcc, S.p3, T.p3);
+  else
+    poisson_vel_fmm_interactions_3d(c, T.x, T.y, T.z, S.x, S.y, S.z, q, sol[0], sol[1], sol[2], S.inside, T.inside,
+                                    w_src, w_tgt[0], w_tgt[1], w_tgt[2], fpp, fpc, fcp, fcc, S.p3, T.p3);
+
+  const int deg = c.interp_degree;
+  const int nchild = c.dim == 2 ? 4 : 8;
+  auto child_of = [&](int i, int j) {
+    if (c.dim == 2) {
+      const TreePanel_2d& P = T.hp2(i);
+      const int ch[4] = {P.child1, P.child2, P.child3, P.child4};
+      return ch[j];
+    }
+    const TreePanel_3d& P = T.hp3(i);
+    const int ch[8] = {P.child1, P.child2, P.child3, P.child4, P.child5, P.child6, P.child7, P.child8};
+    return ch[j];
+  };
+  // One parallel_for per level (a level's children are distinct panels), as
+  // the reference's downward pass launches its functors.
+  auto down = [&](const auto& p2c, const auto& l2p) {
+    for (int lev = 0; lev < T.info.levels - 1; ++lev) {
+      std::vector<int> ij;
+      for (int i = T.info.level_start[lev]; i < T.info.level_start[lev + 1]; ++i)
+        if (needed[i] && !is_leaf_panel(h, T, i))
+          for (int j = 0; j < nchild; ++j)
+            if (needed[child_of(i, j)]) ij.push_back(i * nchild + j);
+      Kokkos::parallel_for((int)ij.size(), [&](int k) { p2c(ij[k] / nchild, ij[k] % nchild); });
+    }
+    std::vector<int> ls;
+    for (int i = 0; i < Pt; ++i)
+      if (sampled[i]) ls.push_back(i);
+    Kokkos::parallel_for((int)ls.size(), [&](int k) { l2p(ls[k]); });
+  };
+  if (c.dim == 2)
+    down(parent_to_child_2d(T.p2, w_tgt[0], deg), leaf_to_point_2d(T.x, T.y, sol[0], w_tgt[0], T.p2, T.inside, deg));
+  else if (kind == 0)
+    down(parent_to_child_3d(T.p3, w_tgt[0], deg),
+         leaf_to_point_3d(T.x, T.y, T.z, sol[0], w_tgt[0], T.p3, T.inside, deg));
+  else
+    down(parent_to_child_3d_3(T.p3, w_tgt[0], w_tgt[1], w_tgt[2], deg),
+         leaf_to_point_3d_3(T.x, T.y, T.z, sol[0], sol[1], sol[2], w_tgt[0], w_tgt[1], w_tgt[2], T.p3, T.inside,
+                            deg));
+  for (int k = 0; k < ncomp; ++k) std::memcpy(out + (size_t)k * T.n, sol[k].data(), sizeof(double) * T.n);
+  return 0;
+}
+
 // Direct sum with the reference's functors (src/direct_sum_impl.hpp), over
 // all nt x ns pairs through an MDRangePolicy, as the examples do
 // (examples/example_poisson_3d.cpp:165). kind 0 = potential, 1 = 3-D velocity.
@@ -375,8 +488,9 @@ int btkref_direct(int dim, int kind, int nt, const double* tx, const double* ty,
 
 // Timed, strided samples of each phase of a 3-D solve (kind 0 potential,
 // 1 velocity), for the CPU baseline. Every `stride`-th work item of each
-// phase is run through the reference's own functor, under the OpenMP
-// parallel_for of the shim. Per phase p (0 base_pots, 1 child_to_parent,
+// phase (denser for phases with fewer than 8 items per thread per stride) is
+// run through the reference's own functor, under the OpenMP parallel_for of
+// the shim. Per phase p (0 base_pots, 1 child_to_parent,
 // 2 pp, 3 pc, 4 cp, 5 cc, 6 parent_to_child, 7 leaf_to_point):
 //   sec[p]   = wall seconds of the sample,
 //   scale[p] = full-phase work / sampled work (kernel evaluations for 2..5,
@@ -396,11 +510,17 @@ int btkref_time_sample_3d(void* p, int kind, int stride, const double* charges, 
   view_reall wx("ptw", T.info.panel_count, ipc), wy("ptwy", T.info.panel_count, ipc), wz("ptwz", T.info.panel_count, ipc);
   view_real s0("s0", T.n), s1("s1", T.n), s2("s2", T.n);
   double eps = c.ker_eps;
+  // A phase with few work items is sampled more densely (at least 8 items
+  // per thread, or all of them), so the sample keeps every thread busy as
+  // the full phase does; scale[] follows the items actually run.
+  const int min_items = 8 * Kokkos::num_threads();
+  auto stride_of = [&](int count) { return std::max(1, std::min(stride, count / std::max(1, min_items))); };
   auto strided = [&](int count, auto&& f, double& sampled) {
-    int m = (count + stride - 1) / stride;
+    const int st = stride_of(count);
+    int m = (count + st - 1) / st;
     sampled = m;
     auto t0 = std::chrono::steady_clock::now();
-    Kokkos::parallel_for(m, [&](int k) { f(k * stride); });
+    Kokkos::parallel_for(m, [&](int k) { f(k * st); });
     return seconds_since(t0);
   };
   double sampled = 0;
@@ -427,10 +547,11 @@ int btkref_time_sample_3d(void* p, int kind, int stride, const double* charges, 
     const view_interact_host& L = *lists[type];
     int count = L.extent_int(0);
     double full = 0, part = 0;
+    const int st = stride_of(count);
     for (int i = 0; i < count; ++i) {
       double e = pair_evals(L, type, i);
       full += e;
-      if (i % stride == 0) part += e;
+      if (i % st == 0) part += e;
     }
     view_interact dL = *dlists[type];
     double sec_t = 0;

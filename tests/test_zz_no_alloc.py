@@ -73,8 +73,9 @@ def test_limit_and_empty_sources(lib):
 
 
 def _pool_high_water(reset):
+    import torch
     from cuda.bindings import driver, runtime as rt
-    err, pool = rt.cudaDeviceGetDefaultMemPool(0)
+    err, pool = rt.cudaDeviceGetDefaultMemPool(torch.cuda.current_device())
     assert err == rt.cudaError_t.cudaSuccess
     attr = rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh
     if reset:
