@@ -78,11 +78,15 @@ struct InteractParams {
   // BTK_ERR_DEVICE_TIMEOUT and leaves); 0 gives up at the first wait (tests
   // of the error path). In-flight copies are always drained with kDrainLimit.
   uint32_t wait_limit;
-  // The last n_audit_items items (kItemAudit) are handed out at every
-  // audit_every-th ticket instead of after the others (0: in array order), so
-  // the FP64 audit items share the SMs with the FP32 work of the solve.
+  // FP64 audit items (kItemAudit) items[n_items, n_items + n_audit_items),
+  // handed out by their own counter *audit_ticket. Blocks [0, audit_blocks)
+  // start on the audit items and the others on the rest; a block whose queue
+  // runs dry moves to the other one, so the audit shares the SMs with the
+  // solve from the start (its FP64 work runs beside FP32 work) and neither
+  // queue leaves SMs idle at its end.
   int n_audit_items;
-  int audit_every;
+  int audit_blocks;
+  int* audit_ticket;
 };
 constexpr uint32_t kWaitLimitDefault = 1u << 22;
 constexpr uint32_t kDrainLimit = 1u << 22;

@@ -28,15 +28,21 @@ namespace {
 constexpr int kChunk = 256;     // sources per shared-memory chunk (8 KB of double4)
 constexpr int kStages = 3;      // ring depth
 
-// Work item of a ticket. With p.audit_every = k > 0 the n_audit_items audit
-// items (stored last) take tickets k-1, 2k-1, ...; the other items keep their
-// order in the remaining tickets (a bijection onto [0, n_items) while
-// n_audit_items * k <= n_items).
-__device__ __forceinline__ int item_of_ticket(const InteractParams& p, int t) {
-  const int k = p.audit_every, na = p.n_audit_items;
-  if (k <= 0 || na <= 0) return t;
-  if ((t + 1) % k == 0 && (t + 1) / k <= na) return p.n_items - na + (t + 1) / k - 1;
-  return t - min(na, t / k);
+// Next work item of a block (thread 0 only): from its own queue, else from
+// the other one; -1 when both are empty. audit: the block's current queue.
+__device__ __forceinline__ int next_item(const InteractParams& p, bool& audit, bool& moved) {
+  for (;;) {
+    if (audit) {
+      const int t = p.n_audit_items > 0 ? atomicAdd(p.audit_ticket, 1) : p.n_audit_items;
+      if (t < p.n_audit_items) return p.n_items + t;
+    } else {
+      const int t = atomicAdd(p.ticket, 1);
+      if (t < p.n_items) return t;
+    }
+    if (moved) return -1;
+    moved = true;
+    audit = !audit;
+  }
 }
 
 template <int DIM, int KIND>
@@ -51,7 +57,7 @@ struct KernelTraits {
 //   VEL  3-D: sum w (t-s) / R^2
 //   FIELD 3-D: sum w / R, sum w (t-s) / R^3;  2-D: sum w log R^2, sum w (t-s)/R^2
 // with R^2 = |t-s|^2 + eps^2.
-template <int DIM, int KIND, bool GUARD>
+template <int DIM, int KIND, bool GUARD, bool NEWTON = false>
 __device__ __forceinline__ void eval_fp64(double tx, double ty, double tz, const double4& s, double eps2,
                                           double* acc) {
   const double dx = tx - s.x, dy = ty - s.y;
@@ -72,7 +78,7 @@ __device__ __forceinline__ void eval_fp64(double tx, double ty, double tz, const
       acc[1] = fma(dy, g, acc[1]);
       acc[2] = fma(dz, g, acc[2]);
     } else {
-      const double ri = GUARD ? rsqrt_fp64_guarded(r2) : rsqrt_fp64(r2);
+      const double ri = GUARD ? rsqrt_fp64_guarded(r2) : (NEWTON ? rsqrt_fp64_newton(r2) : rsqrt_fp64(r2));
       if (KIND == BTK_KIND_POT) {
         acc[0] = fma(s.w, ri, acc[0]);
       } else {
@@ -111,13 +117,14 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
   int pe = 0, poff = 0;
   uint32_t issued = 0;  // global chunk index of the next issue (thread 0)
 
+  bool audit_queue = (int)blockIdx.x < p.audit_blocks, moved = false;  // thread 0's queue state
   while (true) {
     __syncthreads();  // every thread has read the previous ticket
-    if (tid == 0) s_item = atomicAdd(p.ticket, 1);
+    if (tid == 0) s_item = next_item(p, audit_queue, moved);
     __syncthreads();
     const int it = s_item;
-    if (it >= p.n_items || s_abort) break;
-    const WorkItem w = p.items[item_of_ticket(p, it)];
+    if (it < 0 || s_abort) break;
+    const WorkItem w = p.items[it];
     if (w.t_count <= 0 || w.s_total <= 0) continue;  // unused tile of a per-pair-degree item block
     const int n_chunks = (w.s_total + kChunk - 1) / kChunk;
 
@@ -358,13 +365,14 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
   int pe = 0, poff = 0;
   uint32_t issued = 0;
 
+  bool audit_queue = (int)blockIdx.x < p.audit_blocks, moved = false;  // thread 0's queue state
   while (true) {
     __syncthreads();  // every thread has read the previous ticket
-    if (tid == 0) s_item = atomicAdd(p.ticket, 1);
+    if (tid == 0) s_item = next_item(p, audit_queue, moved);
     __syncthreads();
     const int it = s_item;
-    if (it >= p.n_items || s_abort) break;
-    const WorkItem w = p.items[item_of_ticket(p, it)];
+    if (it < 0 || s_abort) break;
+    const WorkItem w = p.items[it];
     if (w.t_count <= 0 || w.s_total <= 0) continue;  // unused tile of a per-pair-degree item block
     const int n_chunks = (w.s_total + kChunk - 1) / kChunk;
     const float thr = fmaxf(w.hx, fmaxf(w.hy, w.hz));  // near sources at least this far from the box: FP32 path
@@ -400,8 +408,9 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
 
     if (w.flags & kItemAudit) {
       // The audit's direct sum, in FP64 like the reference's
-      // (src/direct_sum_impl.hpp:34-94): absolute coordinates, the FP64
-      // reciprocal square root, FP64 sums. Sources are read from the FP64
+      // (src/direct_sum_impl.hpp:34-94): absolute coordinates, an FP64
+      // reciprocal square root (one Newton step from the FP32 seed, relative
+      // error <~ 1e-12), FP64 sums. Sources are read from the FP64
       // stage itself, so a stage is refilled only after the next chunk's
       // barrier (every thread has finished it): chunk c - 1 + kStages is
       // issued at chunk c, one barrier per chunk.
@@ -428,16 +437,20 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
         if (tid == 0 && c >= 1 && c - 1 + kStages < n_chunks) issue(c - 1 + kStages);
         const int cnt = min(kChunk, w.s_total - c * kChunk);
         const double4* sb = sbuf[stage];
-        if (nu == 2) {
+        if (p.eps2 < 1.1754943508222875e-38) {  // r^2 may leave the FP32 normal range: guarded
+          for (int j = 0; j < cnt; ++j)
+            for (int u = 0; u < nu; ++u) eval_fp64<DIM, KIND, true>(ax[u], ay[u], az[u], sb[j], p.eps2, a64[u]);
+        } else if (nu == 2) {
 #pragma unroll 2
           for (int j = 0; j < cnt; ++j) {
             const double4 sj = sb[j];
-            eval_fp64<DIM, KIND, true>(ax[0], ay[0], az[0], sj, p.eps2, a64[0]);
-            eval_fp64<DIM, KIND, true>(ax[1], ay[1], az[1], sj, p.eps2, a64[1]);
+            eval_fp64<DIM, KIND, false, true>(ax[0], ay[0], az[0], sj, p.eps2, a64[0]);
+            eval_fp64<DIM, KIND, false, true>(ax[1], ay[1], az[1], sj, p.eps2, a64[1]);
           }
         } else if (nu == 1) {
 #pragma unroll 2
-          for (int j = 0; j < cnt; ++j) eval_fp64<DIM, KIND, true>(ax[0], ay[0], az[0], sb[j], p.eps2, a64[0]);
+          for (int j = 0; j < cnt; ++j)
+            eval_fp64<DIM, KIND, false, true>(ax[0], ay[0], az[0], sb[j], p.eps2, a64[0]);
         }
       }
       if (s_abort) break;

@@ -554,14 +554,14 @@ struct InteractCtx {
   int* d_ticket_status = nullptr;  // [0] ticket, [1] status
   const double4* d_T4a = nullptr;  // audit targets and outputs (kItemAudit items)
   Ptr4 aout{};
-  int n_audit_items = 0;  // the last n_audit_items of the n_items are audit items
-  int audit_every = 0;    // ... handed out at every audit_every-th ticket (0: last)
+  int n_audit_items = 0;  // audit items follow the n_items in d_items
+  int audit_blocks = 0;   // blocks that start on the audit items
   uint32_t wait_limit = kWaitLimitDefault;
 };
 
 btk_status run_interactions(const InteractCtx& C, const double4* S4, const double4* T4, const int* T_out,
                             Ptr4 out, Ptr4 ptw, cudaStream_t st, cudaEvent_t e0 = nullptr, cudaEvent_t e1 = nullptr) {
-  if (C.n_items == 0) return BTK_OK;
+  if (C.n_items + C.n_audit_items == 0) return BTK_OK;
   InteractParams p{};
   p.items = C.d_items;
   p.n_items = C.n_items;
@@ -581,12 +581,14 @@ btk_status run_interactions(const InteractCtx& C, const double4* S4, const doubl
   p.status = C.d_ticket_status + 1;
   p.wait_limit = C.wait_limit;
   p.n_audit_items = C.n_audit_items;
-  p.audit_every = C.audit_every;
+  p.audit_ticket = C.d_ticket_status + 2;
   const bool guard = p.eps2 < 1.1754943508222875e-38;
   int per_sm = interact_blocks_per_sm(C.dim, C.kind, C.precision, guard);
   if (per_sm <= 0) per_sm = 1;
-  const int grid = std::min(C.n_items, num_sms() * per_sm);
+  const int grid = std::min(C.n_items + C.n_audit_items, num_sms() * per_sm);
+  p.audit_blocks = std::min(C.audit_blocks, grid);
   BTK_CUDA(cudaMemsetAsync(C.d_ticket_status, 0, sizeof(int), st));
+  if (C.n_audit_items > 0) BTK_CUDA(cudaMemsetAsync(C.d_ticket_status + 2, 0, sizeof(int), st));
   if (e0) BTK_CUDA(cudaEventRecord(e0, st));
   BTK_CUDA(launch_interact(C.dim, C.kind, C.precision, guard, p, grid, st));
   if (e1) BTK_CUDA(cudaEventRecord(e1, st));
@@ -652,7 +654,7 @@ struct btk_plan {
   int* d_T_out = nullptr;
   double* d_psw = nullptr;
   double* d_ptw = nullptr;  // ncomp x Pt x ipc
-  int* d_ticket_status = nullptr;
+  int* d_ticket_status = nullptr;  // [0] ticket, [1] device status, [2] audit ticket
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool timed = false;
 
@@ -1240,8 +1242,8 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
   P->ictx.kind = P->kind;
   P->ictx.precision = P->precision;
   P->ictx.eps = P->eps;
-  BTK_TRY(A.alloc(&P->d_ticket_status, 2));
-  BTK_CUDA(cudaMemsetAsync(P->d_ticket_status, 0, 2 * sizeof(int), st));
+  BTK_TRY(A.alloc(&P->d_ticket_status, 3));  // ticket, status, audit ticket
+  BTK_CUDA(cudaMemsetAsync(P->d_ticket_status, 0, 3 * sizeof(int), st));
   P->ictx.d_ticket_status = P->d_ticket_status;
   BTK_TRY(A.alloc(&P->d_psw, (size_t)Ps * P->ipc));
   BTK_TRY(A.alloc(&P->d_ptw, (size_t)P->ncomp * Pt * P->ipc));
@@ -1670,19 +1672,16 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
     BTK_TRY(run_downward(T, P->ncomp, P->d_T4, w, o, st));
     return BTK_OK;
   };
-  // The audit (FP64 direct sum at the sampled targets) runs as work items of
-  // the solve's own launch.
+  // The audit (FP64 direct sum at the sampled targets) runs in the solve's
+  // own interaction launch: its items have their own queue, which two blocks
+  // per SM start on while the others start on the solve's items (measured
+  // about 1 ms faster than queueing the audit after them).
   BTK_CUDA(launch_gather(P->n_audit, P->d_audit_orig, xt, yt, P->dim == 3 ? zt : nullptr, nullptr, P->d_audit_T4, st));
   BTK_CUDA(cudaMemsetAsync(P->d_audit_out, 0, sizeof(double) * (size_t)P->ncomp * std::max(P->n_audit, 1), st));
   BTK_CUDA(cudaMemsetAsync(P->d_audit_sums, 0, 2 * sizeof(double), st));
   InteractCtx with_audit = P->ictx;
-  with_audit.n_items = P->n_items_main + P->n_audit_items;
   with_audit.n_audit_items = P->n_audit_items;
-  {
-    const char* sp = getenv("BTK_AUDIT_SPREAD");
-    if (sp && atoi(sp) > 0 && P->n_audit_items > 0)
-      with_audit.audit_every = with_audit.n_items / P->n_audit_items;
-  }
+  with_audit.audit_blocks = P->precision == BTK_PREC_MIXED ? 2 * num_sms() : 0;
   with_audit.d_T4a = P->d_audit_T4;
   for (int c = 0; c < P->ncomp; ++c) with_audit.aout.p[c] = P->d_audit_out + (size_t)c * P->n_audit;
   BTK_TRY(solve(with_audit));
@@ -2074,8 +2073,8 @@ static btk_status interactions_dropin(int dim, int kind, const btk_run_config* c
   C.n_items = (int)W.items.size();
   BTK_TRY(A.upload(&C.d_items, W.items));
   BTK_TRY(A.upload(&C.d_entries, W.entries));
-  BTK_TRY(A.alloc(&C.d_ticket_status, 2));
-  BTK_CUDA(cudaMemsetAsync(C.d_ticket_status, 0, 2 * sizeof(int), st));
+  BTK_TRY(A.alloc(&C.d_ticket_status, 3));
+  BTK_CUDA(cudaMemsetAsync(C.d_ticket_status, 0, 3 * sizeof(int), st));
   BTK_TRY(run_interactions(C, S4, T4, T_out, out, ptw, st));
   return check_status_word(C.d_ticket_status + 1, st);
 }

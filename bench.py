@@ -153,20 +153,58 @@ def reference_tree(points, threads):
 def reference_sample(rt, q, target_seconds):
     """Strided, timed samples of the reference's own functors (OpenMP build).
     Potential + gradient = the reference's potential pass plus its gradient-type
-    (velocity) pass over the same pairs. Returns dict(value, est_solve_s, ...)."""
+    (velocity) pass over the same pairs. Returns dict(value, est_solve_s,
+    sampled_s = wall seconds of the sample, ...)."""
+    t0 = time.perf_counter()
     # calibrate the stride on a very sparse sample
     cal = 4096
     sec, scale, ev = rt.time_sample_3d(0, cal, q)
     est_full = float(np.sum(sec * scale))
     stride = max(1, int(np.ceil(2 * est_full / max(target_seconds, 1e-3))))
-    total_s, sampled_s, evals = 0.0, 0.0, 0.0
+    total_s, evals = 0.0, 0.0
     for kind in (0, 1):
         sec, scale, ev = rt.time_sample_3d(kind, stride, q)
         total_s += float(np.sum(sec * scale))
-        sampled_s += float(np.sum(sec))
         evals = float(ev[1])
-    return {"value": evals / total_s, "est_solve_s": total_s, "sampled_s": sampled_s, "stride": stride,
-            "evals": evals}
+    return {"value": evals / total_s, "est_solve_s": total_s, "sampled_s": time.perf_counter() - t0,
+            "stride": stride, "evals": evals}
+
+
+VALIDATION_POINTS = 65536
+
+
+def reference_validation(threads):
+    """The sampled estimate against one whole, unsampled reference solve
+    (potential pass + velocity pass, the fixed downward pass) of the same
+    workload family at N = 65,536 (3-D uniform cube, n = 8, theta 0.7, leaf
+    2000): est_solve_s / full_solve_s."""
+    from barytreek_b200 import datagen
+    from oracle import RefLib
+    ref = RefLib(threads=threads)
+    pts, q = datagen.uniform_box(SEED, VALIDATION_POINTS, 3, 0.0, 1.0)
+    rt = ref.create(3, pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS)
+    t0 = time.perf_counter()
+    rt.solve(0, q, fixed=True)
+    rt.solve(1, q, fixed=True)
+    full = time.perf_counter() - t0
+    est = reference_sample(rt, q, 1.0)
+    return {"points": VALIDATION_POINTS, "full_solve_s": full, "est_solve_s": est["est_solve_s"],
+            "validated_ratio": est["est_solve_s"] / full}
+
+
+def reference_config1(threads):
+    """BASELINE configuration 1 in full through the reference: 2-D, N = 65,536
+    uniform in [-1,1]^2, n = 8, theta 0.7, leaf 500, potential (all leaves on
+    the last level: the unmodified downward pass)."""
+    from barytreek_b200 import datagen
+    from oracle import RefLib
+    ref = RefLib(threads=threads)
+    pts, q = datagen.uniform_box(SEED, 65536, 2, -1.0, 1.0)
+    rt = ref.create(2, pts, degree=8, cluster_size=500, theta=0.7, eps=EPS)
+    t0 = time.perf_counter()
+    rt.solve(0, q, fixed=False)
+    return {"workload": "2-D potential, N=65536 uniform [-1,1]^2, n=8, theta=0.7, leaf 500, plain FP64",
+            "full_solve_ms": 1e3 * (time.perf_counter() - t0), "leaves_on_last_level": rt.leaves_on_last_level_only()}
 
 
 def run_reference(args, world, rank):
@@ -178,25 +216,30 @@ def run_reference(args, world, rank):
         return {"impl": "reference", "unavailable": "oracle/_ref/libbtkref.so not built (reference tree absent at build)"}
     pts, q = datagen.uniform_box(SEED, N_POINTS, 3, 0.0, 1.0)
     cores = cpu_cores()
-    per_step = float(os.environ.get("BTK_REF_STEP_SECONDS", "6"))
+    per_step = float(os.environ.get("BTK_REF_STEP_SECONDS", "5"))
     rt = reference_tree(pts, cores)
-    vals, ests = [], []
+    vals, ests, walls = [], [], []
     for i in range(args.warmup + args.steps):
         r = reference_sample(rt, q, per_step)
         if i >= args.warmup:
             vals.append(r["value"])
             ests.append(r["est_solve_s"])
+            walls.append(r["sampled_s"])
     value = statistics.median(vals)
-    sample = (f"every {r['stride']}-th work item of each phase (base_pots, child_to_parent, PP, PC, CP, CC, "
-              f"parent_to_child, leaf_to_point) of the potential pass and of the velocity pass, timed and scaled by "
-              f"work; {r['sampled_s']:.1f} s of CPU work per step")
+    val = reference_validation(cores)
+    sample = (f"one step = every {r['stride']}-th work item of each phase (base_pots, child_to_parent, PP, PC, CP, "
+              f"CC, parent_to_child, leaf_to_point; at least 8 items per thread) of the potential pass and of the "
+              f"velocity pass, timed; interactions/s = the whole solve's interactions / the work-scaled sample time")
     return {"metric": METRIC, "value": value, "unit": "interactions/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(ests), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64)",
             "impl": "reference",
-            "config": {"workload": workload_name(2, 0), "parallelism": "OpenMP host threads"},
+            "config": {"workload": workload_name(2, 0), "parallelism": "OpenMP host threads",
+                       "step": "a bounded sample of the solve (see cpu_baseline.sample)"},
             "cpu_baseline": {"value": value, "unit": "interactions/s", "cores": cores, "kind": "reference",
-                             "sample": sample},
+                             "sample": sample, "est_solve_s": statistics.median(ests),
+                             "validated_ratio": val["validated_ratio"], "validation": val},
+            "configs": {"cfg1_2d_65k": reference_config1(cores)},
             "e2e": {"value": value, "unit": "interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -205,26 +248,45 @@ def flush_l2(buf):
     buf.add_(1.0)
 
 
-def direct_check(tc, q, kind, m=10000):
+def direct_check(tc, q, kind, m=10000, eps=None):
+    """FP64 direct sum (btk_direct_sum) at m seeded targets: (indices, values)."""
     import torch
     from barytreek_b200 import _lib
     L = _lib.load()
+    m = min(m, tc.nt)
     idx = np.sort(np.random.default_rng(12345).choice(tc.nt, m, replace=False))
     t = [torch.from_numpy(np.ascontiguousarray(c[idx])).cuda() for c in tc.targets]
     out = torch.empty((tc.ncomp, m), dtype=torch.float64, device="cuda")
     qd = torch.from_numpy(np.ascontiguousarray(q)).cuda()
     s = tc._s
-    _lib.check(L.btk_direct_sum(3, kind, EPS, m, _lib.ptr(t[0]), _lib.ptr(t[1]), _lib.ptr(t[2]), tc.ns,
-                                _lib.ptr(s[0]), _lib.ptr(s[1]), _lib.ptr(s[2]), _lib.ptr(qd), _lib.ptr(out), None))
+    z = (lambda a: _lib.ptr(a[2])) if tc.dim == 3 else (lambda a: None)
+    _lib.check(L.btk_direct_sum(tc.dim, kind, EPS if eps is None else eps, m, _lib.ptr(t[0]), _lib.ptr(t[1]), z(t),
+                                tc.ns, _lib.ptr(s[0]), _lib.ptr(s[1]), z(s), _lib.ptr(qd), _lib.ptr(out), None))
     return idx, out.cpu().numpy()
 
 
-def load_traffic(key):
-    path = os.path.join(ROOT, "profiles", "traffic.json")
-    try:
-        return json.load(open(path)).get(key)
-    except Exception:
-        return None
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def event_ms(fn, flush):
+    """Device time of fn() on the current stream (L2 flushed before)."""
+    import torch
+    flush_l2(flush)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    r = fn()
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1), r
+
+
+# DRAM bytes (read + write) of one launch of the headline form's interaction
+# kernel at the full workload, from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum; profiles/k_interact_mixed_learned_1m_traffic.md gives
+# the command). None when the workload differs from the captured one.
+TRAFFIC_BYTES = {}
 
 
 class Form:
@@ -267,6 +329,14 @@ class Form:
 
 
 TOL = 1e-6
+# HBM roofline denominator: MEASURED_PEAKS.json (driver-written) when present,
+# else the pool's earlier copy-bandwidth measurement.
+try:
+    HBM_PEAK_GBS = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    HBM_PEAK_SOURCE = "MEASURED_PEAKS.json hbm_gbs (measured)"
+except Exception:
+    HBM_PEAK_GBS = 6650.0
+    HBM_PEAK_SOURCE = "fallback 6.65 TB/s (earlier copy measurement on this pool)"
 
 
 def time_form(form, qd, flush, args, world, local):
@@ -308,6 +378,8 @@ def run_native(args, world, rank, local):
         headline = "mixed"
     names = (["plain", "mixed", "learned", "plain_cc", "mixed_cc"] if headline == "learned"
              else sorted({"plain", headline}))
+    if args.forms:
+        names = [n for n in names if n in args.forms.split(",") or n == headline]
     results, forms = {}, {}
     for name in names:
         t0 = time.time()
@@ -316,8 +388,20 @@ def run_native(args, world, rank, local):
         setup = time.time() - t0
         results[name] = time_form(forms[name], qd, flush, args, world, local)
         results[name]["setup_s"] = setup
-    plain_evals = forms["plain"].tc.evals()
+    plain_evals = (forms["plain"].tc if "plain" in forms else
+                   btk_plan_for_count(pts, kind)).evals()
     H = results[headline]
+    cold = None
+    if headline == "learned":
+        # the first solve on a fresh plan: the adaptive per-pair tolerance at
+        # its starting point (0.05 tol), no solve before it to settle it
+        fresh = Form("learned", pts, args)
+        torch.cuda.synchronize()
+        ms, _ = event_ms(lambda: fresh.step(qd), flush)
+        rep0 = fresh.report
+        cold = {"ms": ms, "audit_rel_l2": rep0["audit_rel_l2"], "fell_back": rep0["fell_back"],
+                "pair_tol": rep0["pair_tol"], "evals_far": rep0["evals_far"]}
+        fresh.tc.close()
     # plan set-up of the headline form with the trees and lists built on the
     # GPU (what a caller with moving points pays per rebuild), against the
     # host-built set-up timed above
@@ -377,9 +461,14 @@ def run_native(args, world, rank, local):
         acc[name] = float(np.linalg.norm(o - ds) / np.linalg.norm(ds))
     per_comp = [float(np.linalg.norm(H["out"].cpu().numpy()[c, idx] - ds[c]) / np.linalg.norm(ds[c]))
                 for c in range(ds.shape[0])]
-    peak = ctypes.c_double()
+    peak, peak64 = ctypes.c_double(), ctypes.c_double()
     fp32 = headline != "plain"
     _lib.check(L.btk_measure_pipe_peak(1 if fp32 else 0, ctypes.byref(peak), None))
+    _lib.check(L.btk_measure_pipe_peak(0, ctypes.byref(peak64), None))
+    # the FP64 and FP32 rates the SM count and clock give (64 and 128 FMA lanes per SM)
+    sm_clock_ghz = H["clocks"]["sm_mhz"] / 1e3 if H["clocks"].get("sm_mhz") else 1.965
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    spec = {"fp32_tflops": n_sm * 128 * 2 * sm_clock_ghz / 1e3, "fp64_tflops": n_sm * 64 * 2 * sm_clock_ghz / 1e3}
     kernel_ms = H["kernel_ms"]
     flops = FLOPS_PER_EVAL[kind] * H["evals"]
     achieved = flops / (kernel_ms * 1e-3) / 1e12
@@ -403,10 +492,13 @@ def run_native(args, world, rank, local):
                       "speedup_vs_plain_fp64": results["plain"]["ms"] / r["ms"]} for n, r in results.items()},
         "roofline": {"bound": "fp32" if fp32 else "fp64", "achieved": achieved, "peak": peak.value,
                      "unit": "TFLOP/s", "frac": achieved / peak.value,
-                     "traffic": load_traffic(f"{kname}_k{kind}_cfg2"), "kernel": f"{kname} (persistent PP/PC/CP/CC)",
+                     "traffic": TRAFFIC_BYTES.get((kname, headline, kind, N_POINTS)),
+                     "kernel": f"{kname} (persistent PP/PC/CP/CC)",
                      "kernel_ms": kernel_ms, "flops_per_launch": flops,
                      "peak_source": "measured live: btk_measure_pipe_peak FMA-chain probe on this GPU "
-                                    f"({'FP32' if fp32 else 'FP64'} pipe)"},
+                                    f"({'FP32' if fp32 else 'FP64'} pipe)",
+                     "frac_of_spec": achieved / spec["fp32_tflops" if fp32 else "fp64_tflops"],
+                     "spec_peaks": spec, "measured_fp64_tflops": peak64.value},
         "e2e": {"value": e2e_value, "unit": "interactions/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_total / args.steps},
         "gpu_launches": H["launches"],
@@ -419,30 +511,147 @@ def run_native(args, world, rank, local):
         r = forms["learned"].report
         line["learned"] = {k: r[k] for k in ("audit_rel_l2", "audit_targets", "fell_back", "evals_near", "evals_far",
                                              "ms_select", "ms_solve", "ms_kernel", "degree_hist", "pair_tol")}
-        # the audit's direct sum runs as items of the same launch
+        # The audit's FP64 direct sum runs as items of the same launch. On this
+        # GPU FP64 and FP32 work on one SM add up (FP64 at half the FP32 rate),
+        # so the launch's roofline time is FP32 flops / FP32 peak + FP64 flops /
+        # FP64 peak; achieved is given in FP32-equivalent TFLOP/s (FP64 flops
+        # scaled by the measured FP32/FP64 peak ratio).
         audit_evals = r["audit_targets"] * N_POINTS
         line["learned"]["evals_audit"] = audit_evals
-        flops = FLOPS_PER_EVAL[kind] * (H["evals"] + audit_evals)
-        achieved = flops / (kernel_ms * 1e-3) / 1e12
-        line["roofline"].update({"achieved": achieved, "frac": achieved / peak.value, "flops_per_launch": flops})
+        flops64 = FLOPS_PER_EVAL[kind] * audit_evals
+        equiv = flops + flops64 * peak.value / peak64.value
+        achieved = equiv / (kernel_ms * 1e-3) / 1e12
+        line["roofline"].update({"achieved": achieved, "frac": achieved / peak.value, "flops_per_launch": flops,
+                                 "fp64_audit_flops_per_launch": flops64, "unit": "TFLOP/s (FP32-equivalent)",
+                                 "frac_of_spec": (flops / spec["fp32_tflops"] + flops64 / spec["fp64_tflops"])
+                                 / 1e12 / (kernel_ms * 1e-3)})
+        line["learned"]["cold_first_solve"] = cold
+    updown = updown_rates(forms.get("plain"), results.get("plain"), kind)
+    if updown:
+        line["roofline"]["updown"] = updown
+    if not args.no_configs:
+        line["configs"] = run_configs(args, flush)
     if batch_line is not None:
         line["batch"] = batch_line
     if world == 1 and not args.no_cpu_baseline:
         from oracle import RefLib
         if RefLib.available():
             r = reference_sample(reference_tree(pts, cpu_cores()), q,
-                                 float(os.environ.get("BTK_CPU_BASELINE_SECONDS", "12")))
+                                 float(os.environ.get("BTK_CPU_BASELINE_SECONDS", "10")))
             line["cpu_baseline"] = {
                 "value": r["value"], "unit": "interactions/s", "cores": cpu_cores(), "kind": "reference",
                 "sample": (f"reference functors (OpenMP, Kokkos-API shim build) on every {r['stride']}-th work item "
-                           f"of every phase of the potential and velocity passes, scaled by work; "
-                           f"{r['sampled_s']:.1f} s of CPU work"),
+                           f"of every phase (at least 8 per thread) of the potential and velocity passes, scaled by "
+                           f"work; {r['sampled_s']:.1f} s of CPU work"),
                 "est_solve_s": r["est_solve_s"]}
+            val = reference_validation(cpu_cores())
+            line["cpu_baseline"].update({"validated_ratio": val["validated_ratio"], "validation": val})
         else:
             line["cpu_baseline"] = None
     for fm in forms.values():
         fm.tc.close()
     return line
+
+
+def btk_plan_for_count(pts, kind):
+    """The plain fixed-degree plan of the workload (for its interaction count)."""
+    import barytreek_b200 as btk
+    return btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=kind)
+
+
+def updown_rates(form, result, kind):
+    """Achieved HBM rates of the upward and downward passes of the plain
+    form (device times from btk_plan_last_timing of its last timed solve).
+    Algorithmic bytes: upward = 36 B per source point (x, y, z, q, leaf id)
+    + the proxy source weights written (panels x (n+1)^3 x 8 B); downward =
+    24 B per target point + the leaves' proxy target weights read (leaves x
+    (n+1)^3 x 8 B per component) + 8 B per point per component written."""
+    if form is None or result is None:
+        return None
+    t = result["info"]
+    tree = form.tc.tree_t
+    n, ipc, nc = form.tc.nt, (DEGREE + 1) ** 3, form.tc.ncomp
+    n_leaves = int(np.count_nonzero(tree.panels["is_leaf"]))
+    up = 36 * n + tree.panel_count * ipc * 8
+    down = 24 * n + n_leaves * ipc * 8 * nc + 8 * n * nc
+    return {"upward_ms": t["upward"], "upward_bytes": up, "upward_gbs": up / (t["upward"] * 1e-3) / 1e9,
+            "downward_ms": t["downward"], "downward_bytes": down,
+            "downward_gbs": down / (t["downward"] * 1e-3) / 1e9,
+            "hbm_peak_gbs": HBM_PEAK_GBS, "peak_source": HBM_PEAK_SOURCE,
+            "form": "plain FP64 (upward: gather, leaf moments, child->parent, source proxies; downward: "
+                    "parent->child, leaf->point)"}
+
+
+def run_configs(args, flush):
+    """The other BASELINE configurations at full size on this GPU (seeded
+    synthetic inputs with their shapes and distributions):
+    cfg1: 2-D potential, N = 65,536 uniform in [-1,1]^2, n = 8, theta 0.7, leaf
+          500, plain FP64;
+    cfg4: 3-D potential + gradient, N = 4,194,304 Plummer sphere (scale 0.1,
+          r <= 2), charges U[0,1], leaf 2000, theta 0.7: learned + mixed at
+          tol 1e-6 against plain FP64 at n = 10;
+    cfg5: the reference's 3-D vector kernel, eps 1e-3, N = 2,097,152 on the
+          unit sphere, strengths U[-1,1], leaf 2000, theta 0.8: learned + mixed
+          against plain FP64 at n = 10.
+    Device times (CUDA events, L2 flushed before each solve); errors against
+    the FP64 direct sum at 10,000 seeded targets. The learned form reports its
+    first solve on a fresh plan (cold) and its time after 3 settling solves."""
+    import torch
+
+    import barytreek_b200 as btk
+    from barytreek_b200 import datagen, selector
+    steps = max(1, min(args.steps, 3))
+    out = {}
+
+    def plain_leg(pts, q, kind, eps, theta, degree, leaf):
+        qd = torch.from_numpy(q).cuda()
+        tc = btk.Treecode(pts, degree=degree, cluster_size=leaf, theta=theta, eps=eps, kind=kind, device_tree=True)
+        tc.solve(qd)
+        ms = [event_ms(lambda: tc.solve(qd), flush)[0] for _ in range(steps)]
+        o = tc.solve(qd).cpu().numpy()
+        idx, ds = direct_check(tc, q, kind, eps=eps)
+        r = {"ms": statistics.median(ms), "evaluations": tc.evals(), "rel_l2_vs_direct_10k": rel_l2(o[:, idx], ds)}
+        tc.close()
+        return r, idx, ds
+
+    def learned_leg(pts, q, kind, eps, theta, degree, leaf, idx, ds):
+        qd = torch.from_numpy(q).cuda()
+        sel = selector.Selector.load(kind=kind)
+        tc = btk.Treecode(pts, degree=degree, cluster_size=leaf, theta=theta, eps=eps, kind=kind,
+                          precision=btk.PREC_MIXED, degree_mode=btk._lib.DEGREE_PER_PAIR, degree_min=4,
+                          leaf_far_pairs=True, device_tree=True)
+        cold_ms, (o, rep0) = event_ms(lambda: tc.solve_learned(qd, sel, tol=TOL), flush)
+        for _ in range(2):
+            tc.solve_learned(qd, sel, tol=TOL)
+        ms = []
+        for _ in range(steps):
+            t, (o, rep) = event_ms(lambda: tc.solve_learned(qd, sel, tol=TOL), flush)
+            ms.append(t)
+        r = {"ms": statistics.median(ms), "cold_first_solve_ms": cold_ms, "cold_fell_back": rep0["fell_back"],
+             "cold_audit_rel_l2": rep0["audit_rel_l2"], "audit_rel_l2": rep["audit_rel_l2"],
+             "fell_back": rep["fell_back"], "pair_tol": rep["pair_tol"],
+             "evaluations": rep["evals_near"] + rep["evals_far"],
+             "rel_l2_vs_direct_10k": rel_l2(o.cpu().numpy()[:, idx], ds)}
+        tc.close()
+        return r
+
+    pts, q = datagen.uniform_box(SEED, 65536, 2, -1.0, 1.0)
+    r, _, _ = plain_leg(pts, q, btk.KIND_POT, EPS, 0.7, 8, 500)
+    out["cfg1_2d_65k"] = {"workload": "2-D potential, N=65536 uniform [-1,1]^2, n=8, theta=0.7, leaf 500",
+                          "plain_fp64": r}
+    for key, what, gen, kind, eps, theta in (
+            ("cfg4_plummer_4m", "3-D potential+gradient, N=4194304 Plummer sphere (a=0.1, r<=2), charges U[0,1], "
+             "theta=0.7, leaf 2000, eps 1e-4", lambda: datagen.plummer(SEED, 1 << 22), btk.KIND_FIELD, 1e-4, 0.7),
+            ("cfg5_sphere_2m_vel", "reference 3-D vector kernel, N=2097152 on the unit sphere, strengths U[-1,1], "
+             "theta=0.8, leaf 2000, eps 1e-3", lambda: datagen.sphere_surface(SEED, 1 << 21), btk.KIND_VEL, 1e-3,
+             0.8)):
+        pts, q = gen()
+        plain, idx, ds = plain_leg(pts, q, kind, eps, theta, 10, 2000)
+        learned = learned_leg(pts, q, kind, eps, theta, 10, 2000, idx, ds)
+        learned["speedup_vs_plain_fp64"] = plain["ms"] / learned["ms"]
+        learned["cold_speedup_vs_plain_fp64"] = plain["ms"] / learned["cold_first_solve_ms"]
+        out[key] = {"workload": what, "plain_fp64_n10": plain, "learned_mixed": learned, "tolerance_rel_l2": TOL}
+    return out
 
 
 def run_batch(args, flush):
@@ -529,6 +738,8 @@ def main():
                     help="the form reported as the headline (all cheaper forms are timed beside it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-problems measurement")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations (1, 4, 5)")
+    ap.add_argument("--forms", default="", help="comma list of the forms to time beside the headline (profiling)")
     ap.add_argument("--batch-only", action="store_true", help="only the batched-problems measurement (profiling)")
     ap.add_argument("--batch-problems", type=int, default=256, help="problems in the batch (profiling captures)")
     ap.add_argument("--points", type=int, default=N_POINTS, help="point count (profiling captures only)")
