@@ -7,46 +7,38 @@
 namespace btk {
 
 // ---------------------------------------------------------------------------
-// FP64 reciprocal square root for the pairwise kernels.
+// FP64 reciprocal square root and reciprocal for the pairwise kernels.
 //
-// Seed: the FP32 approximation rsqrt.approx.f32 (one MUFU op) of the FP32
-// number that shares x's exponent and top 20 mantissa bits. The FP32 bit
-// pattern is built from x's high word by integer re-biasing of the exponent
-// (11-bit bias 1023 -> 8-bit bias 127: subtract 896 << 23 after a 3-bit
-// shift), and the FP32 result is widened the same way in reverse. No
-// floating-point conversion instruction is issued.
+// Seed: the FP32 approximation rsqrt.approx.f32 / rcp.approx.f32 (one MUFU op)
+// of the FP32 number that shares x's exponent and top 23 mantissa bits. The
+// FP32 bit pattern is built from x's two words by integer re-biasing of the
+// exponent (11-bit bias 1023 -> 8-bit bias 127: a 3-bit funnel shift of the
+// high word with the top bits of the low word, then + 128 << 23 in the 9-bit
+// field the shift leaves), and the FP32 result is widened the same way in
+// reverse. No floating-point conversion instruction is issued. The seed's
+// relative error e0 is the truncation (<= 2^-23) plus the approximation's
+// own (about 2^-23), so |e0| <~ 2.5e-7.
 //
-// Refinement: with e = 1 - x*y^2, the third-order Householder step for
-// f(y) = y^-2 - x,  y' = y * (1 + e/2 + 3e^2/8), cubes the relative error
-// (|e| <~ 1e-6 from the seed and the truncated mantissa, so |e'| <~ 1e-18,
-// below FP64 rounding). 5 FP64 operations.
+// Refinement: one Newton step, which squares the relative error:
+//   rsqrt: e = 1 - x y^2, y' = y + (y/2) e   -> error 1.5 e0^2 <~ 1e-13 (4 FP64 ops)
+//   rcp:   e = 1 - x y,   y' = y + y e       -> error e0^2 <~ 7e-14     (2 FP64 ops)
+// far below the 1e-12 agreement with the reference that the FP64 path keeps.
 //
 // Domain: x in the FP32 normal range [2^-126, 2^127]. The kernels guarantee it
-// with eps^2 >= 2^-126; callers with smaller eps use rsqrt_fp64_guarded.
+// with eps^2 >= 2^-126; callers with smaller eps use the guarded variants.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double rsqrt_fp64(double x) {
-  const int hi = __double2hiint(x);
-  const float xf = __int_as_float((hi << 3) + 0x40000000);
-  float yf;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
+__device__ __forceinline__ float fp32_seed_arg(double x) {
+  return __int_as_float(__funnelshift_l(__double2loint(x), __double2hiint(x), 3) + 0x40000000);
+}
+__device__ __forceinline__ double fp64_from_seed(float yf) {
   const int yb = __float_as_int(yf);
-  double y = __hiloint2double((yb >> 3) + 0x38000000, yb << 29);
-  const double e = fma(-x, y * y, 1.0);
-  const double p = fma(0.375, e, 0.5);
-  return fma(y * e, p, y);
+  return __hiloint2double((yb >> 3) + 0x38000000, yb << 29);
 }
 
-// The same seed with one Newton step y' = y (1 + e/2), e = 1 - x y^2 (4 FP64
-// operations): relative error 1.5 e0^2 <~ 1e-12 for the seed's |e0| <~ 1e-6.
-// For sums whose accuracy need is far above FP64 rounding (the learned
-// solve's audit, which measures errors of 1e-9 and above).
-__device__ __forceinline__ double rsqrt_fp64_newton(double x) {
-  const int hi = __double2hiint(x);
-  const float xf = __int_as_float((hi << 3) + 0x40000000);
+__device__ __forceinline__ double rsqrt_fp64(double x) {
   float yf;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
-  const int yb = __float_as_int(yf);
-  const double y = __hiloint2double((yb >> 3) + 0x38000000, yb << 29);
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(fp32_seed_arg(x)));
+  const double y = fp64_from_seed(yf);
   const double e = fma(-x, y * y, 1.0);
   return fma(0.5 * y, e, y);
 }
@@ -58,18 +50,13 @@ __device__ __forceinline__ double rsqrt_fp64_guarded(double x) {
   return rsqrt_fp64(x);
 }
 
-// FP64 reciprocal of a positive x in the FP32 normal range: FP32 MUFU seed
-// (same re-biasing as above) and one cubically convergent Newton-type step
-// y' = y + y*(e + e^2), e = 1 - x*y. 4 FP64 operations.
+// FP64 reciprocal of a positive x in the FP32 normal range (seed and Newton
+// step as above).
 __device__ __forceinline__ double rcp_fp64_pos(double x) {
-  const int hi = __double2hiint(x);
-  const float xf = __int_as_float((hi << 3) + 0x40000000);
   float yf;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
-  const int yb = __float_as_int(yf);
-  const double y = __hiloint2double((yb >> 3) + 0x38000000, yb << 29);
-  const double e = fma(-x, y, 1.0);
-  return fma(y, fma(e, e, e), y);
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(fp32_seed_arg(x)));
+  const double y = fp64_from_seed(yf);
+  return fma(y, fma(-x, y, 1.0), y);
 }
 
 __device__ __forceinline__ double rcp_fp64_pos_guarded(double x) {

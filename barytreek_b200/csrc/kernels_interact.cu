@@ -13,7 +13,8 @@
 // Per item, thread 0 streams the item's sources through a STAGES-deep ring of
 // shared-memory chunks with TMA bulk copies (cp.async.bulk, completion on an
 // mbarrier); all 128 threads evaluate their 2 targets against every source of a
-// chunk (broadcast shared-memory reads) and keep the sums in registers. Warp w
+// chunk (broadcast shared-memory reads) and keep the sums in registers. One
+// block barrier per chunk. Warp w
 // owns targets [64 w, 64 w + 64) of a tile; warps whose targets lie past the
 // tile's count skip the arithmetic. Each
 // target's sum is written once at the end of its item, so results need no
@@ -57,7 +58,7 @@ struct KernelTraits {
 //   VEL  3-D: sum w (t-s) / R^2
 //   FIELD 3-D: sum w / R, sum w (t-s) / R^3;  2-D: sum w log R^2, sum w (t-s)/R^2
 // with R^2 = |t-s|^2 + eps^2.
-template <int DIM, int KIND, bool GUARD, bool NEWTON = false>
+template <int DIM, int KIND, bool GUARD>
 __device__ __forceinline__ void eval_fp64(double tx, double ty, double tz, const double4& s, double eps2,
                                           double* acc) {
   const double dx = tx - s.x, dy = ty - s.y;
@@ -78,7 +79,7 @@ __device__ __forceinline__ void eval_fp64(double tx, double ty, double tz, const
       acc[1] = fma(dy, g, acc[1]);
       acc[2] = fma(dz, g, acc[2]);
     } else {
-      const double ri = GUARD ? rsqrt_fp64_guarded(r2) : (NEWTON ? rsqrt_fp64_newton(r2) : rsqrt_fp64(r2));
+      const double ri = GUARD ? rsqrt_fp64_guarded(r2) : rsqrt_fp64(r2);
       if (KIND == BTK_KIND_POT) {
         acc[0] = fma(s.w, ri, acc[0]);
       } else {
@@ -176,8 +177,11 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
         s_fail_chunk = g + c;
         atomicCAS(p.status, 0, (int)BTK_ERR_DEVICE_TIMEOUT);
       }
+      // One barrier per chunk: chunk c has landed for every thread, and every
+      // thread has finished chunk c - 1, whose stage is refilled now.
       __syncthreads();
       if (s_abort) break;
+      if (tid == 0 && c >= 1 && c - 1 + kStages < n_chunks) issue(c - 1 + kStages);
       const int cnt = min(kChunk, w.s_total - c * kChunk);
       const double4* sb = sbuf[stage];
       if (nu == 2) {
@@ -191,8 +195,6 @@ __global__ void __launch_bounds__(kInteractThreads, 4) k_interact_fp64(InteractP
 #pragma unroll 2
         for (int j = 0; j < cnt; ++j) eval_fp64<DIM, KIND, GUARD>(tx[0], ty[0], tz[0], sb[j], p.eps2, acc[0]);
       }
-      __syncthreads();
-      if (tid == 0 && c + kStages < n_chunks) issue(c + kStages);
     }
     if (s_abort) break;
     g += n_chunks;
@@ -408,9 +410,8 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
 
     if (w.flags & kItemAudit) {
       // The audit's direct sum, in FP64 like the reference's
-      // (src/direct_sum_impl.hpp:34-94): absolute coordinates, an FP64
-      // reciprocal square root (one Newton step from the FP32 seed, relative
-      // error <~ 1e-12), FP64 sums. Sources are read from the FP64
+      // (src/direct_sum_impl.hpp:34-94): absolute coordinates, the FP64
+      // reciprocal square root, FP64 sums. Sources are read from the FP64
       // stage itself, so a stage is refilled only after the next chunk's
       // barrier (every thread has finished it): chunk c - 1 + kStages is
       // issued at chunk c, one barrier per chunk.
@@ -444,13 +445,13 @@ __global__ void __launch_bounds__(kInteractThreads, KIND == BTK_KIND_POT ? 5 : 4
 #pragma unroll 2
           for (int j = 0; j < cnt; ++j) {
             const double4 sj = sb[j];
-            eval_fp64<DIM, KIND, false, true>(ax[0], ay[0], az[0], sj, p.eps2, a64[0]);
-            eval_fp64<DIM, KIND, false, true>(ax[1], ay[1], az[1], sj, p.eps2, a64[1]);
+            eval_fp64<DIM, KIND, false>(ax[0], ay[0], az[0], sj, p.eps2, a64[0]);
+            eval_fp64<DIM, KIND, false>(ax[1], ay[1], az[1], sj, p.eps2, a64[1]);
           }
         } else if (nu == 1) {
 #pragma unroll 2
           for (int j = 0; j < cnt; ++j)
-            eval_fp64<DIM, KIND, false, true>(ax[0], ay[0], az[0], sb[j], p.eps2, a64[0]);
+            eval_fp64<DIM, KIND, false>(ax[0], ay[0], az[0], sb[j], p.eps2, a64[0]);
         }
       }
       if (s_abort) break;

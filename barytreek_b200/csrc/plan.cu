@@ -365,7 +365,14 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
   // PP pairs lead every point target's group; count them per target.
   std::vector<int> n_near(Pt, 0);
   for (int i = 0; i < counts[0]; ++i) n_near[lists[0][i].target_panel]++;
-  // Tiles and items.
+  // Tiles and items. A warp evaluates its targets against every source of
+  // its item, whatever the tile's fill, so an item runs for a time set by its
+  // source count: items are cut (long source lists into pieces of at most
+  // max_cost / kTile sources) and ordered (longest first, for the persistent
+  // grid's longest-processing-time schedule) by that duration; tiles with
+  // more targets go first among equal durations.
+  auto tile_duration = [](int64_t st) { return (int64_t)kTile * st; };
+  auto order_key = [](int tc, int64_t st) { return st * (kTile + 1) + tc; };
   int64_t total_cost = W.evals[0] + W.evals[1] + W.evals[2] + W.evals[3];
   const int64_t max_cost =
       std::max<int64_t>((int64_t)kTile * 8192, total_cost / std::max<int64_t>(1, (int64_t)grid_slots * split));
@@ -406,8 +413,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
       const int tn = proxy ? ipc : T.h.point_count[tp];
       int ni = 0;
       for (int a = 0; a < tn; a += kTile) {
-        const int tc = std::min(kTile, tn - a);
-        const int64_t cost = (int64_t)tc * st;
+        const int64_t cost = tile_duration(st);
         const int nsplit = (int)std::min<int64_t>((cost + max_cost - 1) / max_cost, ne);
         if (nsplit <= 1) {
           ++ni;
@@ -494,10 +500,10 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
       int64_t out = itm_off[tp];
       for (int a = 0; a < tn; a += kTile) {
         const int tc = std::min(kTile, tn - a);
-        const int64_t cost = (int64_t)tc * s_total;
+        const int64_t cost = tile_duration(s_total);
         const int nsplit = (int)std::min<int64_t>((cost + max_cost - 1) / max_cost, e1 - e0);
         if (nsplit <= 1) {
-          items[out++] = {cost, item(t0 + a, tc, e0, e1, s_total, proxy ? kItemProxyTargets : 0)};
+          items[out++] = {order_key(tc, s_total), item(t0 + a, tc, e0, e1, s_total, proxy ? kItemProxyTargets : 0)};
           continue;
         }
         // Split the entry range into nsplit pieces of similar source counts.
@@ -506,7 +512,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
         while (k < e1) {
           int kb = k, st = 0;
           while (k < e1 && (st == 0 || st + W.entries[k].s_count <= per)) st += W.entries[k++].s_count;
-          items[out++] = {(int64_t)tc * st, item(t0 + a, tc, kb, k, st, (proxy ? kItemProxyTargets : 0) | kItemAtomic)};
+          items[out++] = {order_key(tc, st), item(t0 + a, tc, kb, k, st, (proxy ? kItemProxyTargets : 0) | kItemAtomic)};
         }
       }
     }

@@ -489,7 +489,8 @@ def run_native(args, world, rank, local):
                    "interactions_plain": plain_evals, "interactions_evaluated": H["evals"]},
         "forms": {n: {"ms_per_step": r["ms"], "interaction_kernel_ms": r["kernel_ms"], "evaluations": r["evals"],
                       "rel_l2_vs_direct_10k": acc[n], "setup_s": r["setup_s"],
-                      "speedup_vs_plain_fp64": results["plain"]["ms"] / r["ms"]} for n, r in results.items()},
+                      "speedup_vs_plain_fp64": results["plain"]["ms"] / r["ms"] if "plain" in results else None}
+                  for n, r in results.items()},
         "roofline": {"bound": "fp32" if fp32 else "fp64", "achieved": achieved, "peak": peak.value,
                      "unit": "TFLOP/s", "frac": achieved / peak.value,
                      "traffic": TRAFFIC_BYTES.get((kname, headline, kind, N_POINTS)),

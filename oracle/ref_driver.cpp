@@ -263,17 +263,23 @@ void btkref_get_lists(void* p, void* all, void* pp, void* pc, void* cp, void* cc
 }  // extern "C"
 
 // Fixed downward pass (see file header): the reference's functors, called on
-// non-leaf parents only (levels 0..L-2, in level order) and on every leaf.
+// non-leaf parents only (levels 0..L-2, one parallel_for per level, as the
+// reference's downward pass launches them) and on every leaf (one
+// parallel_for).
 template <class P2C, class L2P>
 static void fixed_downward(Handle& h, const P2C& p2c, const L2P& l2p) {
   Tree& t = h.tgt;
-  int nchild = h.cfg.dim == 2 ? 4 : 8;
-  for (int lev = 0; lev < t.info.levels - 1; ++lev)
+  const int nchild = h.cfg.dim == 2 ? 4 : 8;
+  for (int lev = 0; lev < t.info.levels - 1; ++lev) {
+    std::vector<int> parents;
     for (int i = t.info.level_start[lev]; i < t.info.level_start[lev + 1]; ++i)
-      if (!is_leaf_panel(h, t, i))
-        for (int j = 0; j < nchild; ++j) p2c(i, j);
+      if (!is_leaf_panel(h, t, i)) parents.push_back(i);
+    Kokkos::parallel_for((int)parents.size() * nchild, [&](int k) { p2c(parents[k / nchild], k % nchild); });
+  }
+  std::vector<int> leaves;
   for (int i = 0; i < t.info.panel_count; ++i)
-    if (is_leaf_panel(h, t, i)) l2p(i);
+    if (is_leaf_panel(h, t, i)) leaves.push_back(i);
+  Kokkos::parallel_for((int)leaves.size(), [&](int k) { l2p(leaves[k]); });
 }
 
 extern "C" {
