@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -1990,124 +1991,310 @@ btk_status btk_solve_host(int dim, int kind, int precision, int degree, int clus
 // Drop-in entry points (reference names and argument order; device pointers)
 // =============================================================================
 
-static btk_status upward_dropin(int dim, const btk_run_config* cfg, const btk_tree_info* info, const double* x,
-                                const double* y, const double* z, const double* q, const void* d_panels, double* psw,
-                                const int* d_leaf_of, int n, cudaStream_t st) {
+// ---- drop-in entry points ---------------------------------------------------
+// The reference-named calls take the tree, leaf rows and interaction lists as
+// the caller's device arrays on every call. What is derived from them (the
+// host tree, the device sides, the work lists and the solve's buffers) is kept
+// between calls in a small cache keyed by the buffers' addresses, counts and
+// run configuration, and validated on every call by a fingerprint of the
+// buffers' contents computed on the device (an order-independent sum of a
+// 64-bit mix of every 32-bit word and its position), so a tree rebuilt in the
+// same buffers is detected and rebuilt. Calls hold one process-wide lock
+// (they synchronise their stream before returning anyway).
+namespace btk {
+namespace {
+
+__global__ void k_fingerprint(const uint32_t* w, long long n, unsigned long long* out) {
+  unsigned long long acc = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long z = (unsigned long long)w[i] * 0x9E3779B97F4A7C15ULL ^ (unsigned long long)i * 0xD6E8FEB86659FD93ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    acc += z ^ (z >> 31);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+struct DevBuf {
+  const void* p;
+  size_t bytes;
+};
+
+// Fingerprints of the buffers (each a multiple of 4 bytes), one per buffer.
+btk_status fingerprints(const std::vector<DevBuf>& bufs, std::vector<unsigned long long>& fp, cudaStream_t st) {
+  static unsigned long long* d_fp[64] = {};
+  static size_t cap[64] = {};
+  int dev = 0;
+  BTK_CUDA(cudaGetDevice(&dev));
+  BTK_CHECK(dev >= 0 && dev < 64, BTK_ERR_UNSUPPORTED, "drop-in cache: device index above 63");
+  if (cap[dev] < bufs.size()) {
+    if (d_fp[dev]) cudaFree(d_fp[dev]);
+    BTK_CUDA(cudaMalloc(&d_fp[dev], sizeof(unsigned long long) * 16));
+    cap[dev] = 16;
+  }
+  BTK_CHECK(bufs.size() <= cap[dev], BTK_ERR_INTERNAL, "drop-in cache: too many buffers");
+  BTK_CUDA(cudaMemsetAsync(d_fp[dev], 0, sizeof(unsigned long long) * bufs.size(), st));
+  for (size_t k = 0; k < bufs.size(); ++k) {
+    const long long n = (long long)(bufs[k].bytes / 4);
+    if (!bufs[k].p || n == 0) continue;
+    count_launch();
+    k_fingerprint<<<num_sms() * 4, 256, 0, st>>>((const uint32_t*)bufs[k].p, n, d_fp[dev] + k);
+    BTK_CUDA(cudaGetLastError());
+  }
+  fp.assign(bufs.size(), 0);
+  BTK_CUDA(cudaMemcpyAsync(fp.data(), d_fp[dev], sizeof(unsigned long long) * bufs.size(), cudaMemcpyDeviceToHost,
+                           st));
+  BTK_CUDA(cudaStreamSynchronize(st));
+  return BTK_OK;
+}
+
+// Key of a cache entry: addresses, counts and configuration values as words.
+using DropinKey = std::vector<long long>;
+
+struct DropinEntry {
+  DropinKey key;
+  std::vector<unsigned long long> fp;
+  std::unique_ptr<Arena> arena;  // on the legacy stream: valid whatever the callers' streams
+  Side T, S;                     // upward/downward use T only; interactions both
+  double4 *S4 = nullptr, *T4 = nullptr, *pts = nullptr;
+  int* T_out = nullptr;
+  InteractCtx ctx;
+  uint64_t last_use = 0;
+};
+
+std::mutex g_dropin_mu;
+std::vector<std::unique_ptr<DropinEntry>> g_dropin;  // at most kDropinEntries
+uint64_t g_dropin_clock = 0;
+constexpr size_t kDropinEntries = 6;
+
+// The entry for key/fp (valid), or a fresh one to build (its key/fp set); the
+// least recently used entry makes room.
+DropinEntry* dropin_lookup(const DropinKey& key, const std::vector<unsigned long long>& fp, bool& fresh) {
+  for (auto& e : g_dropin)
+    if (e->key == key) {
+      e->last_use = ++g_dropin_clock;
+      fresh = e->fp != fp;
+      if (fresh) {  // same buffers, new contents: rebuild in place
+        cudaDeviceSynchronize();
+        e.reset(new DropinEntry());
+        e->key = key;
+        e->fp = fp;
+        e->last_use = g_dropin_clock;
+      }
+      return e.get();
+    }
+  if (g_dropin.size() >= kDropinEntries) {
+    auto lru = std::min_element(g_dropin.begin(), g_dropin.end(),
+                                [](const auto& x, const auto& y) { return x->last_use < y->last_use; });
+    cudaDeviceSynchronize();  // its buffers may still be read by earlier work
+    g_dropin.erase(lru);
+  }
+  g_dropin.emplace_back(new DropinEntry());
+  DropinEntry* e = g_dropin.back().get();
+  e->key = key;
+  e->fp = fp;
+  e->last_use = ++g_dropin_clock;
+  fresh = true;
+  return e;
+}
+
+DropinKey key_of(int what, int dim, const btk_run_config* cfg, std::initializer_list<long long> more) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  DropinKey k = {what, dev, dim, cfg->interp_degree, cfg->fmm_cluster_thresh};
+  k.insert(k.end(), more.begin(), more.end());
+  return k;
+}
+
+btk_status upward_dropin(int dim, const btk_run_config* cfg, const btk_tree_info* info, const double* x,
+                         const double* y, const double* z, const double* q, const void* d_panels, double* psw,
+                         const int* d_leaf_of, int n, cudaStream_t st) {
   BTK_TRY(validate_cfg(cfg, dim));
   BTK_CHECK(info && info->level_start && info->panel_count > 0 && info->levels > 0, BTK_ERR_INVALID_ARGUMENT,
             "upward_pass: bad tree_info");
   BTK_CHECK(n >= 0 && x && y && q && psw && d_leaf_of && (dim == 2 || z), BTK_ERR_INVALID_ARGUMENT,
             "upward_pass: null argument");
-  Side S;
-  std::vector<int> leaf_of;
-  if (dim == 2) {
-    std::vector<btk_panel_2d> hp;
-    BTK_TRY(fetch_panels((const btk_panel_2d*)d_panels, info->panel_count, hp, st));
-    BTK_TRY(fetch(d_leaf_of, n, leaf_of, st));
-    BTK_CUDA(cudaStreamSynchronize(st));
-    host_tree_from_panels(2, hp.data(), info->panel_count, info->level_start, info->levels, S.h);
-  } else {
-    std::vector<btk_panel_3d> hp;
-    BTK_TRY(fetch_panels((const btk_panel_3d*)d_panels, info->panel_count, hp, st));
-    BTK_TRY(fetch(d_leaf_of, n, leaf_of, st));
-    BTK_CUDA(cudaStreamSynchronize(st));
-    host_tree_from_panels(3, hp.data(), info->panel_count, info->level_start, info->levels, S.h);
+  const size_t panel_bytes = dim == 2 ? sizeof(btk_panel_2d) : sizeof(btk_panel_3d);
+  std::lock_guard<std::mutex> lock(g_dropin_mu);
+  DropinKey key = key_of(0, dim, cfg, {(long long)(uintptr_t)d_panels, info->panel_count, info->levels,
+                                       (long long)(uintptr_t)d_leaf_of, n});
+  key.insert(key.end(), info->level_start, info->level_start + info->levels + 1);
+  std::vector<unsigned long long> fp;
+  BTK_TRY(fingerprints({{d_panels, panel_bytes * info->panel_count}, {d_leaf_of, sizeof(int) * (size_t)n}}, fp, st));
+  bool fresh = false;
+  DropinEntry* E = dropin_lookup(key, fp, fresh);
+  if (fresh) {
+    Side& S = E->T;
+    std::vector<int> leaf_of;
+    if (dim == 2) {
+      std::vector<btk_panel_2d> hp;
+      BTK_TRY(fetch_panels((const btk_panel_2d*)d_panels, info->panel_count, hp, st));
+      BTK_TRY(fetch(d_leaf_of, n, leaf_of, st));
+      BTK_CUDA(cudaStreamSynchronize(st));
+      host_tree_from_panels(2, hp.data(), info->panel_count, info->level_start, info->levels, S.h);
+    } else {
+      std::vector<btk_panel_3d> hp;
+      BTK_TRY(fetch_panels((const btk_panel_3d*)d_panels, info->panel_count, hp, st));
+      BTK_TRY(fetch(d_leaf_of, n, leaf_of, st));
+      BTK_CUDA(cudaStreamSynchronize(st));
+      host_tree_from_panels(3, hp.data(), info->panel_count, info->level_start, info->levels, S.h);
+    }
+    E->arena.reset(new Arena(nullptr));
+    Arena& A = *E->arena;
+    btk_status rc = side_layout(S, n, cfg->interp_degree);
+    if (rc == BTK_OK) rc = side_upload(S, A, nullptr, nullptr, cfg->fmm_cluster_thresh);
+    if (rc == BTK_OK) rc = side_perm_from_leaf_of(S, A, leaf_of);
+    if (rc == BTK_OK) rc = A.alloc(&E->pts, (size_t)std::max(n, 1));
+    if (rc == BTK_OK && cudaStreamSynchronize(nullptr) != cudaSuccess) rc = BTK_ERR_CUDA;
+    if (rc != BTK_OK) {
+      E->key.clear();  // never matches: rebuilt on the next call
+      return rc;
+    }
   }
-  BTK_TRY(side_layout(S, n, cfg->interp_degree));
-  Arena A(st);
-  BTK_TRY(side_upload(S, A, nullptr, nullptr, cfg->fmm_cluster_thresh));
-  BTK_TRY(side_perm_from_leaf_of(S, A, leaf_of));
-  double4* pts = nullptr;
-  BTK_TRY(A.alloc(&pts, (size_t)std::max(n, 1)));
-  BTK_CUDA(launch_gather(n, S.d_perm, x, y, dim == 3 ? z : nullptr, q, pts, st));
-  BTK_TRY(run_upward(S, pts, psw, st));
+  BTK_CUDA(launch_gather(n, E->T.d_perm, x, y, dim == 3 ? z : nullptr, q, E->pts, st));
+  BTK_TRY(run_upward(E->T, E->pts, psw, st));
   BTK_CUDA(cudaStreamSynchronize(st));
   return BTK_OK;
 }
 
 template <class PanelT>
-static btk_status interactions_dropin(int dim, int kind, const btk_run_config* cfg, const double* xt, const double* yt,
-                                      const double* zt, const double* xs, const double* ys, const double* zs,
-                                      const double* q, Ptr4 out, const int* inside_s, const int* inside_t,
-                                      const double* psw, Ptr4 ptw, const btk_interact_pair* const dl[4],
-                                      const PanelT* panels_s, const PanelT* panels_t, int nt, int ns, int Pt, int Ps,
-                                      cudaStream_t st) {
+btk_status interactions_dropin(int dim, int kind, const btk_run_config* cfg, const double* xt, const double* yt,
+                               const double* zt, const double* xs, const double* ys, const double* zs, const double* q,
+                               Ptr4 out, const int* inside_s, const int* inside_t, const double* psw, Ptr4 ptw,
+                               const btk_interact_pair* const dl[4], const PanelT* panels_s, const PanelT* panels_t,
+                               int nt, int ns, int Pt, int Ps, cudaStream_t st) {
   BTK_TRY(validate_cfg(cfg, dim));
   BTK_CHECK(nt >= 0 && ns >= 0 && xt && yt && xs && ys && q && psw && inside_s && inside_t && (dim == 2 || (zt && zs)),
             BTK_ERR_INVALID_ARGUMENT, "interactions: null argument");
+  BTK_CHECK(Pt > 0 && Ps > 0 && panels_s && panels_t, BTK_ERR_INVALID_ARGUMENT, "interactions: bad panel arrays");
   const int counts[4] = {cfg->fmm_pp_count, cfg->fmm_pc_count, cfg->fmm_cp_count, cfg->fmm_cc_count};
-  std::vector<PanelT> hpt, hps;
-  std::vector<btk_interact_pair> hl[4];
-  BTK_TRY(fetch_panels(panels_t, Pt, hpt, st));
-  BTK_TRY(fetch_panels(panels_s, Ps, hps, st));
-  for (int t = 0; t < 4; ++t) BTK_TRY(fetch(dl[t], counts[t], hl[t], st));
-  BTK_CUDA(cudaStreamSynchronize(st));
-  Side T, Sown;
-  BTK_CHECK(host_tree_from_panels_nolevels(dim, hpt.data(), Pt, T.h), BTK_ERR_INVALID_ARGUMENT,
-            "target panels are not in level order");
-  BTK_TRY(side_layout(T, nt, cfg->interp_degree));
-  BTK_CHECK(host_tree_from_panels_nolevels(dim, hps.data(), Ps, Sown.h), BTK_ERR_INVALID_ARGUMENT,
-            "source panels are not in level order");
-  BTK_TRY(side_layout(Sown, ns, cfg->interp_degree));
-  Arena A(st);
-  BTK_TRY(side_upload(T, A, nullptr, inside_t, cfg->fmm_cluster_thresh));
-  BTK_TRY(side_upload(Sown, A, nullptr, inside_s, cfg->fmm_cluster_thresh));
-  const Side& S = Sown;
-  const int ipc = S.ipc;
+  for (int t = 0; t < 4; ++t)
+    BTK_CHECK(counts[t] >= 0 && (counts[t] == 0 || dl[t]), BTK_ERR_INVALID_ARGUMENT, "interactions: null list");
+  const size_t thresh = (size_t)cfg->fmm_cluster_thresh;
+  std::lock_guard<std::mutex> lock(g_dropin_mu);
+  const DropinKey key =
+      key_of(1, dim, cfg, {kind, (long long)(uintptr_t)panels_t, (long long)(uintptr_t)panels_s,
+                           (long long)(uintptr_t)inside_t, (long long)(uintptr_t)inside_s,
+                           (long long)(uintptr_t)dl[0], (long long)(uintptr_t)dl[1], (long long)(uintptr_t)dl[2],
+                           (long long)(uintptr_t)dl[3], counts[0], counts[1], counts[2], counts[3], nt, ns, Pt, Ps});
+  std::vector<DevBuf> bufs = {{panels_t, sizeof(PanelT) * Pt}, {inside_t, sizeof(int) * thresh * Pt}};
+  if ((const void*)panels_s != (const void*)panels_t) bufs.push_back({panels_s, sizeof(PanelT) * Ps});
+  if (inside_s != inside_t) bufs.push_back({inside_s, sizeof(int) * thresh * Ps});
+  for (int t = 0; t < 4; ++t) bufs.push_back({dl[t], sizeof(btk_interact_pair) * counts[t]});
+  std::vector<unsigned long long> fp;
+  BTK_TRY(fingerprints(bufs, fp, st));
+  bool fresh = false;
+  DropinEntry* E = dropin_lookup(key, fp, fresh);
+  if (fresh) {
+    auto build = [&]() -> btk_status {
+      std::vector<PanelT> hpt, hps;
+      std::vector<btk_interact_pair> hl[4];
+      BTK_TRY(fetch_panels(panels_t, Pt, hpt, st));
+      BTK_TRY(fetch_panels(panels_s, Ps, hps, st));
+      for (int t = 0; t < 4; ++t) BTK_TRY(fetch(dl[t], counts[t], hl[t], st));
+      BTK_CUDA(cudaStreamSynchronize(st));
+      Side &T = E->T, &S = E->S;
+      BTK_CHECK(host_tree_from_panels_nolevels(dim, hpt.data(), Pt, T.h), BTK_ERR_INVALID_ARGUMENT,
+                "target panels are not in level order");
+      BTK_TRY(side_layout(T, nt, cfg->interp_degree));
+      BTK_CHECK(host_tree_from_panels_nolevels(dim, hps.data(), Ps, S.h), BTK_ERR_INVALID_ARGUMENT,
+                "source panels are not in level order");
+      BTK_TRY(side_layout(S, ns, cfg->interp_degree));
+      E->arena.reset(new Arena(nullptr));
+      Arena& A = *E->arena;
+      BTK_TRY(side_upload(T, A, nullptr, inside_t, cfg->fmm_cluster_thresh));
+      BTK_TRY(side_upload(S, A, nullptr, inside_s, cfg->fmm_cluster_thresh));
+      const int ipc = S.ipc;
+      const int nct = (int)T.clusters.size(), ncs = (int)S.clusters.size();
+      BTK_TRY(A.alloc(&E->S4, (size_t)ns + (size_t)ncs * ipc + 1));
+      BTK_TRY(A.alloc(&E->T4, (size_t)nt + (size_t)nct * ipc + 1));
+      BTK_TRY(A.alloc(&E->T_out, (size_t)nt + (size_t)nct * ipc + 1));
+      const btk_interact_pair* hlp[4] = {hl[0].data(), hl[1].data(), hl[2].data(), hl[3].data()};
+      const bool guard = cfg->ker_eps * cfg->ker_eps < 1.1754943508222875e-38;
+      const int slots = num_sms() * std::max(1, interact_blocks_per_sm(dim, kind, BTK_PREC_FP64, guard));
+      WorkLists W;
+      BTK_TRY(build_work(T, S, hlp, counts, slots, W));
+      InteractCtx& C = E->ctx;
+      C.dim = dim;
+      C.kind = kind;
+      C.precision = BTK_PREC_FP64;
+      C.eps = cfg->ker_eps;
+      C.n_items = (int)W.items.size();
+      BTK_TRY(A.upload(&C.d_items, W.items));
+      BTK_TRY(A.upload(&C.d_entries, W.entries));
+      BTK_TRY(A.alloc(&C.d_ticket_status, 3));
+      BTK_CUDA(cudaMemsetAsync(C.d_ticket_status, 0, 3 * sizeof(int), nullptr));
+      BTK_CUDA(cudaStreamSynchronize(nullptr));  // the uploads read host vectors that go out of scope
+      return BTK_OK;
+    };
+    const btk_status rc = build();
+    if (rc != BTK_OK) {
+      E->key.clear();
+      return rc;
+    }
+  }
+  const Side &T = E->T, &S = E->S;
   const int nct = (int)T.clusters.size(), ncs = (int)S.clusters.size();
-  // Sources: sorted points + cluster proxies carrying the modified charges.
-  double4 *S4 = nullptr, *T4 = nullptr;
-  int* T_out = nullptr;
-  BTK_TRY(A.alloc(&S4, (size_t)ns + (size_t)ncs * ipc + 1));
-  BTK_TRY(A.alloc(&T4, (size_t)nt + (size_t)nct * ipc + 1));
-  BTK_TRY(A.alloc(&T_out, (size_t)nt + (size_t)nct * ipc + 1));
-  BTK_CUDA(launch_gather(ns, S.d_perm, xs, ys, dim == 3 ? zs : nullptr, q, S4, st));
-  BTK_CUDA(launch_src_proxies(dim, S.degree, ncs, S.d_clusters, S.d_nodes_shift, psw, S4 + ns, st));
-  BTK_CUDA(launch_gather(nt, T.d_perm, xt, yt, dim == 3 ? zt : nullptr, nullptr, T4, st));
-  if (nt) BTK_CUDA(cudaMemcpyAsync(T_out, T.d_perm, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
-  BTK_CUDA(launch_tgt_proxies(dim, T.degree, nct, T.d_clusters, T.d_nodes_shift, T4 + nt, T_out + nt, st));
-  const btk_interact_pair* hlp[4] = {hl[0].data(), hl[1].data(), hl[2].data(), hl[3].data()};
-  const bool guard = cfg->ker_eps * cfg->ker_eps < 1.1754943508222875e-38;
-  const int slots = num_sms() * std::max(1, interact_blocks_per_sm(dim, kind, BTK_PREC_FP64, guard));
-  WorkLists W;
-  BTK_TRY(build_work(T, S, hlp, counts, slots, W));
-  InteractCtx C;
-  C.dim = dim;
-  C.kind = kind;
-  C.precision = BTK_PREC_FP64;
-  C.eps = cfg->ker_eps;
-  C.n_items = (int)W.items.size();
-  BTK_TRY(A.upload(&C.d_items, W.items));
-  BTK_TRY(A.upload(&C.d_entries, W.entries));
-  BTK_TRY(A.alloc(&C.d_ticket_status, 3));
-  BTK_CUDA(cudaMemsetAsync(C.d_ticket_status, 0, 3 * sizeof(int), st));
-  BTK_TRY(run_interactions(C, S4, T4, T_out, out, ptw, st));
-  return check_status_word(C.d_ticket_status + 1, st);
+  // Per call: sources (sorted points + cluster proxies carrying this call's
+  // modified charges) and targets (sorted points + cluster proxy points).
+  BTK_CUDA(launch_gather(ns, S.d_perm, xs, ys, dim == 3 ? zs : nullptr, q, E->S4, st));
+  BTK_CUDA(launch_src_proxies(dim, S.degree, ncs, S.d_clusters, S.d_nodes_shift, psw, E->S4 + ns, st));
+  BTK_CUDA(launch_gather(nt, T.d_perm, xt, yt, dim == 3 ? zt : nullptr, nullptr, E->T4, st));
+  if (nt) BTK_CUDA(cudaMemcpyAsync(E->T_out, T.d_perm, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st));
+  BTK_CUDA(launch_tgt_proxies(dim, T.degree, nct, T.d_clusters, T.d_nodes_shift, E->T4 + nt, E->T_out + nt, st));
+  BTK_CUDA(cudaMemsetAsync(E->ctx.d_ticket_status + 1, 0, sizeof(int), st));
+  BTK_TRY(run_interactions(E->ctx, E->S4, E->T4, E->T_out, out, ptw, st));
+  return check_status_word(E->ctx.d_ticket_status + 1, st);
 }
 
 template <class PanelT>
-static btk_status downward_dropin(int dim, int ncomp, const btk_run_config* cfg, const btk_tree_info* info,
-                                  const double* x, const double* y, const double* z, Ptr4 out, const PanelT* panels,
-                                  Ptr4 ptw, const int* inside, int n, cudaStream_t st) {
+btk_status downward_dropin(int dim, int ncomp, const btk_run_config* cfg, const btk_tree_info* info, const double* x,
+                           const double* y, const double* z, Ptr4 out, const PanelT* panels, Ptr4 ptw,
+                           const int* inside, int n, cudaStream_t st) {
   BTK_TRY(validate_cfg(cfg, dim));
   BTK_CHECK(info && info->level_start && info->panel_count > 0 && info->levels > 0, BTK_ERR_INVALID_ARGUMENT,
             "downward_pass: bad tree_info");
-  BTK_CHECK(n >= 0 && x && y && inside && (dim == 2 || z), BTK_ERR_INVALID_ARGUMENT, "downward_pass: null argument");
-  std::vector<PanelT> hp;
-  BTK_TRY(fetch_panels(panels, info->panel_count, hp, st));
-  BTK_CUDA(cudaStreamSynchronize(st));
-  Side T;
-  host_tree_from_panels(dim, hp.data(), info->panel_count, info->level_start, info->levels, T.h);
-  BTK_TRY(side_layout(T, n, cfg->interp_degree));
-  Arena A(st);
-  BTK_TRY(side_upload(T, A, nullptr, inside, cfg->fmm_cluster_thresh));
-  double4* pts = nullptr;
-  BTK_TRY(A.alloc(&pts, (size_t)std::max(n, 1)));
-  BTK_CUDA(launch_gather(n, T.d_perm, x, y, dim == 3 ? z : nullptr, nullptr, pts, st));
-  BTK_TRY(run_downward(T, ncomp, pts, ptw, out, st));
+  BTK_CHECK(n >= 0 && x && y && inside && panels && (dim == 2 || z), BTK_ERR_INVALID_ARGUMENT,
+            "downward_pass: null argument");
+  std::lock_guard<std::mutex> lock(g_dropin_mu);
+  DropinKey key = key_of(2, dim, cfg, {(long long)(uintptr_t)panels, info->panel_count, info->levels,
+                                       (long long)(uintptr_t)inside, n});
+  key.insert(key.end(), info->level_start, info->level_start + info->levels + 1);
+  std::vector<unsigned long long> fp;
+  BTK_TRY(fingerprints({{panels, sizeof(PanelT) * info->panel_count},
+                        {inside, sizeof(int) * (size_t)cfg->fmm_cluster_thresh * info->panel_count}},
+                       fp, st));
+  bool fresh = false;
+  DropinEntry* E = dropin_lookup(key, fp, fresh);
+  if (fresh) {
+    auto build = [&]() -> btk_status {
+      std::vector<PanelT> hp;
+      BTK_TRY(fetch_panels(panels, info->panel_count, hp, st));
+      BTK_CUDA(cudaStreamSynchronize(st));
+      Side& T = E->T;
+      host_tree_from_panels(dim, hp.data(), info->panel_count, info->level_start, info->levels, T.h);
+      BTK_TRY(side_layout(T, n, cfg->interp_degree));
+      E->arena.reset(new Arena(nullptr));
+      BTK_TRY(side_upload(T, *E->arena, nullptr, inside, cfg->fmm_cluster_thresh));
+      BTK_TRY(E->arena->alloc(&E->pts, (size_t)std::max(n, 1)));
+      BTK_CUDA(cudaStreamSynchronize(nullptr));
+      return BTK_OK;
+    };
+    const btk_status rc = build();
+    if (rc != BTK_OK) {
+      E->key.clear();
+      return rc;
+    }
+  }
+  BTK_CUDA(launch_gather(n, E->T.d_perm, x, y, dim == 3 ? z : nullptr, nullptr, E->pts, st));
+  BTK_TRY(run_downward(E->T, ncomp, E->pts, ptw, out, st));
   BTK_CUDA(cudaStreamSynchronize(st));
   return BTK_OK;
 }
+
+}  // namespace
+}  // namespace btk
 
 extern "C" {
 

@@ -532,6 +532,7 @@ def run_native(args, world, rank, local):
         line["roofline"]["updown"] = updown
     if not args.no_configs:
         line["configs"] = run_configs(args, flush)
+        line["dropin"] = run_dropin(pts, q, flush, max(1, min(args.steps, 3)))
     if batch_line is not None:
         line["batch"] = batch_line
     if world == 1 and not args.no_cpu_baseline:
@@ -653,6 +654,83 @@ def run_configs(args, flush):
         learned["cold_speedup_vs_plain_fp64"] = plain["ms"] / learned["cold_first_solve_ms"]
         out[key] = {"workload": what, "plain_fp64_n10": plain, "learned_mixed": learned, "tolerance_rel_l2": TOL}
     return out
+
+
+def run_dropin(pts, q, flush, steps):
+    """The reference-named call sequence of a solve (examples/
+    example_poisson_3d.cpp:142-156: upward_pass_3d -> poisson_fmm_interactions_3d
+    -> downward_pass_3d) through the drop-in entry points on device arrays in
+    the reference's layouts, for the headline workload's potential (the drop-in
+    interactions are the reference's potential kernel), against the plan path's
+    plain FP64 potential solve. Each drop-in call synchronises its stream, as
+    the reference's Kokkos calls fence; times are wall-clock around the three
+    calls (after one warm-up sequence, which builds the cached plan state)."""
+    import torch
+
+    import barytreek_b200 as btk
+    from barytreek_b200 import _lib
+    L = _lib.load()
+    cfg = btk.make_run_config(3, DEGREE, LEAF, THETA, EPS)
+    tree = btk.tree_construction(cfg, pts)
+    lists = btk.split_interactions(cfg, btk.dual_tree_traversal(cfg, tree))
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    X = [dev(a) for a in pts]
+    Q = dev(q)
+    panels, leaf_of, inside = dev(tree.panels.view(np.uint8)), dev(tree.point_leaf_panel), dev(
+        tree.panel_points_inside)
+    Ld = [dev(l.view(np.uint8)) if len(l) else None for l in lists]
+    n, P, ipc = len(q), tree.panel_count, cfg.interp_point_count
+    ti = tree.tree_info()
+    p = _lib.ptr
+    psw = torch.empty((P, ipc), dtype=torch.float64, device="cuda")
+    ptw = torch.empty((P, ipc), dtype=torch.float64, device="cuda")
+    sol = torch.empty(n, dtype=torch.float64, device="cuda")
+
+    def sequence():
+        psw.zero_()
+        ptw.zero_()
+        sol.zero_()
+        _lib.check(L.btk_upward_pass_3d(ctypes.byref(cfg), ctypes.byref(ti), p(X[0]), p(X[1]), p(X[2]), p(Q),
+                                        p(panels), p(psw), p(leaf_of), n, None))
+        _lib.check(L.btk_poisson_fmm_interactions_3d(
+            ctypes.byref(cfg), p(X[0]), p(X[1]), p(X[2]), p(X[0]), p(X[1]), p(X[2]), p(Q), p(sol), p(inside),
+            p(inside), p(psw), p(ptw), *[p(l) if l is not None else None for l in Ld], p(panels), p(panels), n, n,
+            P, P, None))
+        _lib.check(L.btk_downward_pass_3d(ctypes.byref(cfg), ctypes.byref(ti), p(X[0]), p(X[1]), p(X[2]), p(sol),
+                                          p(panels), p(ptw), p(inside), n, None))
+
+    t0 = time.perf_counter()
+    sequence()
+    torch.cuda.synchronize()
+    first = time.perf_counter() - t0
+    ms = []
+    for _ in range(steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sequence()
+        torch.cuda.synchronize()
+        ms.append(1e3 * (time.perf_counter() - t0))
+    out_dropin = sol.cpu().numpy()
+    tc = btk.Treecode(pts, degree=DEGREE, cluster_size=LEAF, theta=THETA, eps=EPS, kind=btk.KIND_POT)
+    tc.solve(Q)
+    plan_ms = []
+    for _ in range(steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        o = tc.solve(Q)
+        torch.cuda.synchronize()
+        plan_ms.append(1e3 * (time.perf_counter() - t0))
+    agree = rel_l2(out_dropin, o.cpu().numpy()[0])
+    tc.close()
+    return {"workload": "3D Coulomb potential (the reference's potential path), N=%d, n=%d, theta=%g, leaf %d, "
+                        "plain FP64" % (n, DEGREE, THETA, LEAF),
+            "calls": "btk_upward_pass_3d -> btk_poisson_fmm_interactions_3d -> btk_downward_pass_3d",
+            "ms_per_solve": statistics.median(ms), "first_call_ms": 1e3 * first,
+            "plan_path_ms_per_solve": statistics.median(plan_ms),
+            "ratio_to_plan_path": statistics.median(ms) / statistics.median(plan_ms),
+            "rel_l2_vs_plan_path": agree}
 
 
 def run_batch(args, flush):

@@ -248,3 +248,61 @@ def test_invalid_arguments_are_rejected(lib):
     assert e.value.status == _lib.ERR_UNSUPPORTED
     with pytest.raises(btk.BtkError):
         btk.Treecode(pts, degree=4, cluster_size=50, kind=1, precision=7)
+
+
+def _dropin_sequence(lib, cfg, ti, X, Q, panels, leaf_of, inside, L, n, P, ipc):
+    """upward_pass_3d -> poisson_fmm_interactions_3d -> downward_pass_3d on
+    fresh outputs; returns the potential."""
+    import torch
+    from barytreek_b200 import _lib
+    p = _lib.ptr
+    psw = torch.zeros((P, ipc), dtype=torch.float64, device="cuda")
+    ptw = torch.zeros((P, ipc), dtype=torch.float64, device="cuda")
+    sol = torch.zeros(n, dtype=torch.float64, device="cuda")
+    Lp = [p(l) if l is not None else None for l in L]
+    _lib.check(lib.btk_upward_pass_3d(ctypes.byref(cfg), ctypes.byref(ti), p(X[0]), p(X[1]), p(X[2]), p(Q),
+                                      p(panels), p(psw), p(leaf_of), n, None))
+    _lib.check(lib.btk_poisson_fmm_interactions_3d(
+        ctypes.byref(cfg), p(X[0]), p(X[1]), p(X[2]), p(X[0]), p(X[1]), p(X[2]), p(Q), p(sol), p(inside), p(inside),
+        p(psw), p(ptw), *Lp, p(panels), p(panels), n, n, P, P, None))
+    _lib.check(lib.btk_downward_pass_3d(ctypes.byref(cfg), ctypes.byref(ti), p(X[0]), p(X[1]), p(X[2]), p(sol),
+                                        p(panels), p(ptw), p(inside), n, None))
+    return sol.cpu().numpy()
+
+
+def test_dropin_cache_reuse_and_rebuild(oracle, lib):
+    """The drop-in entry points keep what they derive from the caller's tree
+    and lists between calls: a second call on the same buffers reuses it, and
+    a tree rebuilt into the same buffers (points scaled by 1.25: the same
+    counts and lists, other panel boxes) is detected and rebuilt. Each result
+    matches the oracle to 1e-12."""
+    import barytreek_b200 as btk
+    pts, _, q = make(3, 3000, seed=52)
+    cfg = btk.make_run_config(3, 5, 80, 0.7, 1e-4)
+    results = []
+    bufs = None
+    for scale in (1.0, 1.0, 1.25):
+        p_s = tuple(c * scale for c in pts)
+        tree = btk.tree_construction(cfg, p_s)
+        lists = btk.split_interactions(cfg, btk.dual_tree_traversal(cfg, tree))
+        host = [tree.panels.view(np.uint8), tree.point_leaf_panel, tree.panel_points_inside] + \
+               [l.view(np.uint8) for l in lists]
+        if bufs is None:
+            bufs = [_dev(a) for a in host]
+        else:  # rebuilt into the same device buffers
+            import torch
+            for b, a in zip(bufs, host):
+                assert b.numel() == a.size
+                b.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+        X = [_dev(a) for a in p_s]
+        out = _dropin_sequence(lib, cfg, tree.tree_info(), X, _dev(q), bufs[0], bufs[1], bufs[2], bufs[3:],
+                               len(q), tree.panel_count, cfg.interp_point_count)
+        d = {"dim": 3, "degree": 5, "eps": 1e-4, "thresh": 80, "targets": p_s, "sources": p_s,
+             "panels_t": tree.panels, "panels_s": tree.panels, "level_start_t": tree.level_start,
+             "level_start_s": tree.level_start, "leaf_of_s": tree.point_leaf_panel,
+             "inside_t": tree.panel_points_inside, "inside_s": tree.panel_points_inside,
+             "pp": lists[0], "pc": lists[1], "cp": lists[2], "cc": lists[3]}
+        ref = oracle.solve(d, 0, q)["out"][0]
+        assert rel(out, ref) <= TOL, scale
+        results.append(out)
+    assert rel(results[1], results[0]) <= 1e-14
