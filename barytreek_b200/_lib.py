@@ -139,6 +139,7 @@ SIGNATURES = {
     "btk_cc_operator_groups": [_ci, _vp, _ci, _vp, _ci, _vp, _ci, _vp, _vp],
     "btk_plan_execute": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "btk_plan_last_timing": [_vp, _vp],
+    "btk_dropin_cache_clear": [],
     "btk_plan_set_wait_limit": [_vp, ctypes.c_longlong],
     "btk_plan_audit_targets": [_vp, _vp, _vp],
     "btk_solve_host": [_ci, _ci, _ci, _ci, _ci, _cd, _cd, _ci, _vp, _vp, _vp, _vp, _vp, _vp],

@@ -2298,6 +2298,16 @@ btk_status downward_dropin(int dim, int ncomp, const btk_run_config* cfg, const 
 
 extern "C" {
 
+btk_status btk_dropin_cache_clear(void) {
+  std::lock_guard<std::mutex> lock(btk::g_dropin_mu);
+  if (!btk::g_dropin.empty()) {
+    BTK_CUDA(cudaDeviceSynchronize());  // work issued by earlier calls may still read the entries
+    btk::g_dropin.clear();
+    BTK_CUDA(cudaDeviceSynchronize());
+  }
+  return BTK_OK;
+}
+
 btk_status btk_upward_pass_2d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
                               const double* ycos, const double* charges, const btk_panel_2d* blfmm_panels,
                               double* proxy_source_weights, const int* point_leaf_panel, int point_count,

@@ -196,6 +196,17 @@ btk_status btk_split_interactions(const btk_interact_pair* interaction_list, int
  *  - degrees above btk_max_degree() are rejected (the reference clamps the
  *    namelist value to 10 before any call). */
 
+/* The drop-in entry points below keep what they derive from the caller's
+ * tree, leaf rows and interaction lists (the host tree, the device-side tree
+ * arrays, the interaction work lists and their buffers) between calls, keyed
+ * by those device buffers' addresses, the counts and the run configuration,
+ * and checked on every call against a fingerprint of the buffers' contents
+ * (computed on the device), so a tree rebuilt into the same buffers is noticed
+ * and rebuilt. Calls are serialised by one process-wide lock. The cache holds
+ * device memory until btk_dropin_cache_clear (no reference counterpart),
+ * which frees it. */
+btk_status btk_dropin_cache_clear(void);
+
 /* src/upward_pass.hpp:7 */
 btk_status btk_upward_pass_2d(const btk_run_config* cfg, const btk_tree_info* info, const double* xcos,
                               const double* ycos, const double* charges, const btk_panel_2d* blfmm_panels,
