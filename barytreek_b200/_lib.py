@@ -61,7 +61,8 @@ class PlanDesc(ctypes.Structure):
                 ("pc_list", ctypes.c_void_p), ("cp_list", ctypes.c_void_p), ("cc_list", ctypes.c_void_p),
                 ("kind", ctypes.c_int), ("precision", ctypes.c_int), ("degree_mode", ctypes.c_int),
                 ("degree_min", ctypes.c_int), ("work_split", ctypes.c_int), ("cc_operators", ctypes.c_int),
-                ("leaf_far_pairs", ctypes.c_int), ("leaf_far_theta", ctypes.c_double)]
+                ("leaf_far_pairs", ctypes.c_int), ("leaf_far_theta", ctypes.c_double),
+                ("tile_targets", ctypes.c_int)]
 
 
 class PlanStats(ctypes.Structure):

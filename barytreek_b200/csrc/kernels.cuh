@@ -91,9 +91,11 @@ struct InteractParams {
 constexpr uint32_t kWaitLimitDefault = 1u << 22;
 constexpr uint32_t kDrainLimit = 1u << 22;
 
-constexpr int kInteractThreads = 128;
+// Work items hold at most kTile targets; a plan's items are tiles of `tile`
+// targets (256 or 128), run by interaction blocks of tile / 2 threads (two
+// targets per thread, 64 per warp).
 constexpr int kTargetsPerThread = 2;
-constexpr int kTile = kInteractThreads * kTargetsPerThread;  // targets per work item
+constexpr int kTile = 256;
 
 // ---- launchers (return cudaGetLastError of the launch) -----------------------
 cudaError_t launch_panel_geometry(int dim, int degree, int P, const DevPanel* panels, const double* ucos_shift,
@@ -118,8 +120,8 @@ cudaError_t launch_l2p(int dim, int degree, int ncomp, int n_leaves, const int* 
                        const int* point_count, const double4* pts, const int* perm, const double* nodes_interp,
                        Ptr4 ptw, Ptr4 out, cudaStream_t s);
 cudaError_t launch_interact(int dim, int kind, int precision, bool guard, const InteractParams& p, int grid,
-                            cudaStream_t s);
-int interact_blocks_per_sm(int dim, int kind, int precision, bool guard);
+                            cudaStream_t s, int tile);
+int interact_blocks_per_sm(int dim, int kind, int precision, bool guard, int tile);
 cudaError_t launch_direct(int dim, int kind, double eps, int nt, const double* xt, const double* yt,
                           const double* zt, int ns, const double4* src, double* out, cudaStream_t s);
 
@@ -241,6 +243,7 @@ cudaError_t launch_resolve(int dim, int n_pc, const int* pc_entry, const int* pc
                            const int* cluster_slot_begin_s, const long long* tgt_slot_offset,
                            const int* cluster_slot_begin_t, int slot_d_lo, long long t4_base, long long s4_base,
                            const double* tgt_centre, int n_point_items, WorkItem* items, Entry* entries,
-                           int far_item0, int far_entry0, int* slot_used, cudaStream_t s);  // marks the source slots read
+                           int far_item0, int far_entry0, int* slot_used, int tile,
+                           cudaStream_t s);  // marks the source slots read
 
 }  // namespace btk

@@ -243,7 +243,7 @@ __global__ void k_far_items(int dim, int n_far, int tiles_max, const int* far_ty
                             const int* cluster_slot_begin_t, const long long* src_slot_offset,
                             const int* cluster_slot_begin_s, int slot_d_lo, long long t4_base, long long s4_base,
                             const double* tgt_centre, WorkItem* items, Entry* entries, int far_item0,
-                            int far_entry0, int* slot_used) {
+                            int far_entry0, int* slot_used, int tile) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_far) return;
   const int d = degree[i];
@@ -273,9 +273,9 @@ __global__ void k_far_items(int dim, int n_far, int tiles_max, const int* far_ty
   const long long t0 = t4_base + tgt_slot_offset[tslot];
   for (int k = 0; k < tiles_max; ++k) {
     WorkItem w{};
-    const int a = k * kTile;
+    const int a = k * tile;
     w.t_begin = (int)(t0 + a);
-    w.t_count = a < ipc_d ? min(kTile, ipc_d - a) : 0;
+    w.t_count = a < ipc_d ? min(tile, ipc_d - a) : 0;
     w.e_begin = far_entry0 + i;
     w.e_end = far_entry0 + i + 1;
     w.s_total = e.s_count;
@@ -327,7 +327,7 @@ cudaError_t launch_resolve(int dim, int n_pc, const int* pc_entry, const int* pc
                            const int* cluster_slot_begin_s, const long long* tgt_slot_offset,
                            const int* cluster_slot_begin_t, int slot_d_lo, long long t4_base, long long s4_base,
                            const double* tgt_centre, int n_point_items, WorkItem* items, Entry* entries,
-                           int far_item0, int far_entry0, int* slot_used, cudaStream_t s) {
+                           int far_item0, int far_entry0, int* slot_used, int tile, cudaStream_t s) {
   if (n_pc > 0) {
     k_resolve_pc<<<(n_pc + 255) / 256, 256, 0, s>>>(dim, n_pc, pc_entry, pc_src_cluster, deg_pc, pc_direct,
                                                     src_slot_offset, cluster_slot_begin_s, slot_d_lo, s4_base,
@@ -342,7 +342,7 @@ cudaError_t launch_resolve(int dim, int n_pc, const int* pc_entry, const int* pc
     k_far_items<<<(n_far + 127) / 128, 128, 0, s>>>(dim, n_far, tiles_max, far_type, far_tgt_cluster, far_src, deg_far,
                                                     tgt_slot_offset, cluster_slot_begin_t, src_slot_offset,
                                                     cluster_slot_begin_s, slot_d_lo, t4_base, s4_base, tgt_centre,
-                                                    items, entries, far_item0, far_entry0, slot_used);
+                                                    items, entries, far_item0, far_entry0, slot_used, tile);
     count_launch();
   }
   return cudaGetLastError();

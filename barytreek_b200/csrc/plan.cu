@@ -260,7 +260,8 @@ int host_threads() {
 
 btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* const lists[4], const int counts[4],
                       int grid_slots, WorkLists& W, const std::vector<long long>* pc_begin = nullptr,
-                      std::vector<int>* pc_entry = nullptr, int split = 8, std::vector<int>* pp_entry = nullptr) {
+                      std::vector<int>* pc_entry = nullptr, int split = 8, std::vector<int>* pp_entry = nullptr,
+                      int tile = kTile) {
   const int ipc = S.ipc;
   const int nt = T.n_points, ns = S.n_points;
   const int Pt = T.h.panel_count, Ps = S.h.panel_count;
@@ -368,15 +369,16 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
   for (int i = 0; i < counts[0]; ++i) n_near[lists[0][i].target_panel]++;
   // Tiles and items. A warp evaluates its targets against every source of
   // its item, whatever the tile's fill, so an item runs for a time set by its
-  // source count: items are cut (long source lists into pieces of at most
-  // max_cost / kTile sources) and ordered (longest first, for the persistent
-  // grid's longest-processing-time schedule) by that duration; tiles with
-  // more targets go first among equal durations.
-  auto tile_duration = [](int64_t st) { return (int64_t)kTile * st; };
-  auto order_key = [](int tc, int64_t st) { return st * (kTile + 1) + tc; };
+  // source count: long source lists are cut into pieces of at most
+  // max_cost / tile sources whatever the tile's fill. Items are ordered by
+  // their evaluations, largest first (the persistent grid's
+  // longest-processing-time schedule; measured faster for the mixed kernel
+  // than ordering by source count).
+  auto tile_duration = [tile](int64_t st) { return (int64_t)tile * st; };
+  auto order_key = [](int tc, int64_t st) { return (int64_t)tc * st; };
   int64_t total_cost = W.evals[0] + W.evals[1] + W.evals[2] + W.evals[3];
   const int64_t max_cost =
-      std::max<int64_t>((int64_t)kTile * 8192, total_cost / std::max<int64_t>(1, (int64_t)grid_slots * split));
+      std::max<int64_t>((int64_t)tile * 8192, total_cost / std::max<int64_t>(1, (int64_t)grid_slots * split));
   // Pass A per target: touching PP sources first (stable), then the other PP
   // sources, then the rest; count its non-empty entries and its items.
   std::vector<int> n_ent(Pt + 1, 0), n_itm(Pt + 1, 0), n_touch(Pt, 0), s_tot(Pt, 0);
@@ -413,7 +415,7 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
       const bool proxy = !T.h.is_leaf[tp];
       const int tn = proxy ? ipc : T.h.point_count[tp];
       int ni = 0;
-      for (int a = 0; a < tn; a += kTile) {
+      for (int a = 0; a < tn; a += tile) {
         const int64_t cost = tile_duration(st);
         const int nsplit = (int)std::min<int64_t>((cost + max_cost - 1) / max_cost, ne);
         if (nsplit <= 1) {
@@ -499,8 +501,8 @@ btk_status build_work(const Side& T, const Side& S, const btk_interact_pair* con
         return w;
       };
       int64_t out = itm_off[tp];
-      for (int a = 0; a < tn; a += kTile) {
-        const int tc = std::min(kTile, tn - a);
+      for (int a = 0; a < tn; a += tile) {
+        const int tc = std::min(tile, tn - a);
         const int64_t cost = tile_duration(s_total);
         const int nsplit = (int)std::min<int64_t>((cost + max_cost - 1) / max_cost, e1 - e0);
         if (nsplit <= 1) {
@@ -564,6 +566,7 @@ struct InteractCtx {
   int n_audit_items = 0;  // audit items follow the n_items in d_items
   int audit_blocks = 0;   // blocks that start on the audit items
   uint32_t wait_limit = kWaitLimitDefault;
+  int tile = kTile;  // targets per work item: 256 (128-thread blocks) or 128 (64-thread blocks)
 };
 
 btk_status run_interactions(const InteractCtx& C, const double4* S4, const double4* T4, const int* T_out,
@@ -590,14 +593,14 @@ btk_status run_interactions(const InteractCtx& C, const double4* S4, const doubl
   p.n_audit_items = C.n_audit_items;
   p.audit_ticket = C.d_ticket_status + 2;
   const bool guard = p.eps2 < 1.1754943508222875e-38;
-  int per_sm = interact_blocks_per_sm(C.dim, C.kind, C.precision, guard);
+  int per_sm = interact_blocks_per_sm(C.dim, C.kind, C.precision, guard, C.tile);
   if (per_sm <= 0) per_sm = 1;
   const int grid = std::min(C.n_items + C.n_audit_items, num_sms() * per_sm);
   p.audit_blocks = std::min(C.audit_blocks, grid);
   BTK_CUDA(cudaMemsetAsync(C.d_ticket_status, 0, sizeof(int), st));
   if (C.n_audit_items > 0) BTK_CUDA(cudaMemsetAsync(C.d_ticket_status + 2, 0, sizeof(int), st));
   if (e0) BTK_CUDA(cudaEventRecord(e0, st));
-  BTK_CUDA(launch_interact(C.dim, C.kind, C.precision, guard, p, grid, st));
+  BTK_CUDA(launch_interact(C.dim, C.kind, C.precision, guard, p, grid, st, C.tile));
   if (e1) BTK_CUDA(cudaEventRecord(e1, st));
   return BTK_OK;
 }
@@ -984,7 +987,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
   {
     const auto t0 = std::chrono::steady_clock::now();
     BTK_TRY(build_work(T, S, lists, counts_static, slots, W, &pc_begin, &pc_entry, P->work_split,
-                       conv.empty() ? nullptr : &pp_entry));
+                       conv.empty() ? nullptr : &pp_entry, P->ictx.tile));
     P->build_ms_work += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   for (int i : conv) {
@@ -1070,7 +1073,7 @@ btk_status plan_build_per_pair(btk_plan* P, const btk_interact_pair* const lists
       const PanelGeom& g = T.h.geom[slot_panels_t[c]];
       centre[3 * c + d] = 0.5 * (g.lo[d] + g.hi[d]);
     }
-  P->tiles_max = (int)((sz(n) + kTile - 1) / kTile);
+  P->tiles_max = (int)((sz(n) + P->ictx.tile - 1) / P->ictx.tile);
   BTK_TRY(A.upload(&P->d_pc_entry, pc_entry));
   BTK_TRY(A.upload(&P->d_pc_src_cluster, pc_src_cluster));
   BTK_TRY(A.upload(&P->d_far_type, far_type));
@@ -1244,7 +1247,11 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
   for (int t = 0; t < 4; ++t) BTK_CHECK(counts[t] >= 0 && (counts[t] == 0 || lists[t]), BTK_ERR_INVALID_ARGUMENT,
                                         "plan: missing interaction list");
   const bool guard = P->eps * P->eps < 1.1754943508222875e-38;
-  const int slots = num_sms() * std::max(1, interact_blocks_per_sm(P->dim, P->kind, P->precision, guard));
+  BTK_CHECK(D->tile_targets == 0 || D->tile_targets == 128 || D->tile_targets == 256, BTK_ERR_INVALID_ARGUMENT,
+            "tile_targets must be 0, 128 or 256");
+  P->ictx.tile = D->tile_targets ? D->tile_targets : kTile;
+  const int slots =
+      num_sms() * std::max(1, interact_blocks_per_sm(P->dim, P->kind, P->precision, guard, P->ictx.tile));
   P->ictx.dim = P->dim;
   P->ictx.kind = P->kind;
   P->ictx.precision = P->precision;
@@ -1289,7 +1296,7 @@ btk_status plan_build(btk_plan* P, const btk_plan_desc* D, cudaStream_t st) {
         counts_w[3] = 0;
       }
     }
-    BTK_TRY(build_work(T, S, lists, counts_w, slots, W, nullptr, nullptr, P->work_split));
+    BTK_TRY(build_work(T, S, lists, counts_w, slots, W, nullptr, nullptr, P->work_split, nullptr, P->ictx.tile));
     P->build_ms_work += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     for (int t = 0; t < 4; ++t) P->evals[t] = W.evals[t];
     if (P->n_cc_tasks > 0) P->evals[3] = (int64_t)counts[3] * P->ipc * P->ipc;
@@ -1413,7 +1420,8 @@ btk_status btk_plan_execute(btk_plan* P, const double* xt, const double* yt, con
                             P->d_far_type, P->d_far_tgt, P->d_far_src, P->d_deg_far, P->d_s_slot_off,
                             P->d_s_cluster_slot_begin, P->d_t_slot_off, P->d_t_cluster_slot_begin, P->degree_min,
                             T.n_points, S.n_points, P->d_tgt_centre, P->n_static_items, P->ictx.d_items,
-                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, P->d_s_slot_used, st));
+                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, P->d_s_slot_used,
+                            P->ictx.tile, st));
     BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
                               S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
                               P->d_s_slot_used, P->d_S4 + S.n_points, st));
@@ -1468,7 +1476,7 @@ namespace {
 // The audit: a fixed, seeded 1% sample of the targets (at least one when
 // there are targets), spread evenly over the index range, and work items for
 // its FP64 direct sum over every source, built on the host at plan creation:
-// tiles of kTile sampled targets x pieces of kAuditPiece consecutive sources
+// tiles of the plan's tile size of sampled targets x pieces of kAuditPiece consecutive sources
 // of the leaf-ordered source array (kItemAudit | kItemAtomic; the interaction
 // kernels evaluate them in FP64 whatever the plan's precision).
 constexpr int kAuditPiece = 4096;
@@ -1487,11 +1495,12 @@ void build_audit_work(const btk_plan* P, int entry_base, AuditWork& W) {
     W.orig[k] = (int)(lo + (int64_t)(z % (uint64_t)std::max<int64_t>(1, hi - lo)));
   }
   for (int s0 = 0; s0 < ns; s0 += kAuditPiece) W.entries.push_back(Entry{s0, std::min(kAuditPiece, ns - s0)});
-  for (int t0 = 0; t0 < na; t0 += kTile)
+  const int tile = P->ictx.tile;
+  for (int t0 = 0; t0 < na; t0 += tile)
     for (int e = 0; e < (int)W.entries.size(); ++e) {
       WorkItem w{};
       w.t_begin = t0;
-      w.t_count = std::min(kTile, na - t0);
+      w.t_count = std::min(tile, na - t0);
       w.e_begin = entry_base + e;
       w.e_end = entry_base + e + 1;
       w.s_total = W.entries[e].s_count;
@@ -1662,7 +1671,8 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
                             P->d_far_type, P->d_far_tgt, P->d_far_src, P->d_deg_far, P->d_s_slot_off,
                             P->d_s_cluster_slot_begin, P->d_t_slot_off, P->d_t_cluster_slot_begin, P->degree_min,
                             T.n_points, S.n_points, P->d_tgt_centre, P->n_static_items, P->ictx.d_items,
-                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, P->d_s_slot_used, st));
+                            P->ictx.d_entries, P->n_static_items, P->n_static_entries, P->d_s_slot_used,
+                            P->ictx.tile, st));
     BTK_CUDA(launch_src_slots(P->dim, P->degree, P->n_src_slots, P->d_s_slot_panel, P->d_s_slot_deg, P->d_s_slot_off,
                               S.d_panels, P->d_psw, P->d_amat, P->d_amat_off, P->d_ucos, P->d_ucos_off,
                               P->d_s_slot_used, P->d_S4 + S.n_points, st));
@@ -2212,7 +2222,7 @@ btk_status interactions_dropin(int dim, int kind, const btk_run_config* cfg, con
       BTK_TRY(A.alloc(&E->T_out, (size_t)nt + (size_t)nct * ipc + 1));
       const btk_interact_pair* hlp[4] = {hl[0].data(), hl[1].data(), hl[2].data(), hl[3].data()};
       const bool guard = cfg->ker_eps * cfg->ker_eps < 1.1754943508222875e-38;
-      const int slots = num_sms() * std::max(1, interact_blocks_per_sm(dim, kind, BTK_PREC_FP64, guard));
+      const int slots = num_sms() * std::max(1, interact_blocks_per_sm(dim, kind, BTK_PREC_FP64, guard, kTile));
       WorkLists W;
       BTK_TRY(build_work(T, S, hlp, counts, slots, W));
       InteractCtx& C = E->ctx;

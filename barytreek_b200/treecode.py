@@ -231,14 +231,16 @@ class Treecode:
     leaf ordering, geometry and interaction work lists. ``cc_operators=True`` applies the CC pairs of
     a fixed-degree plan as shared kernel matrices (pairs grouped by level and lattice offset).
     ``leaf_far_pairs=True`` (per-pair plans) lets the learned degree choice approximate well-separated
-    PP pairs as target points x source-leaf proxies, with the direct evaluation as an option. :meth:`solve` takes
+    PP pairs as target points x source-leaf proxies, with the direct evaluation as an option.
+    ``tile_targets=128`` runs the interaction kernels on tiles of 128 targets (64-thread blocks) instead of 256.
+    :meth:`solve` takes
     charges (numpy or a CUDA tensor) and returns a CUDA tensor
     ``[ncomp, n_targets]`` in the original point order.
     """
 
     def __init__(self, coords, sources=None, *, degree=8, cluster_size=100, theta=0.7, eps=1e-4, kind=KIND_POT,
                  precision=PREC_FP64, degree_mode=_lib.DEGREE_FIXED, degree_min=1, work_split=0, device_tree=False,
-                 cc_operators=False, leaf_far_pairs=False, leaf_far_theta=0.0, device="cuda"):
+                 cc_operators=False, leaf_far_pairs=False, leaf_far_theta=0.0, tile_targets=0, device="cuda"):
         import torch
 
         self.dim = len(coords)
@@ -248,6 +250,7 @@ class Treecode:
         self.cc_operators = bool(cc_operators)
         self.leaf_far_pairs = bool(leaf_far_pairs)
         self.leaf_far_theta = float(leaf_far_theta)
+        self.tile_targets = int(tile_targets)
         self.ncomp = ncomp(self.dim, kind)
         self.cfg = make_run_config(self.dim, degree, cluster_size, theta, eps)
         self.targets = tuple(np.ascontiguousarray(c, np.float64) for c in coords)
@@ -294,6 +297,7 @@ class Treecode:
         d.cc_operators = int(self.cc_operators)
         d.leaf_far_pairs = int(self.leaf_far_pairs)
         d.leaf_far_theta = self.leaf_far_theta
+        d.tile_targets = self.tile_targets
         stream = torch.cuda.current_stream(self.device).cuda_stream
         check(load().btk_plan_create(ctypes.byref(self._plan), ctypes.byref(d), stream))
 

@@ -374,6 +374,10 @@ typedef struct {
    * choice. <= 0: max(fmm_theta, 0.8), the largest MAC parameter the shipped
    * selector was trained on. */
   double leaf_far_theta;
+  /* Targets per interaction work item (no reference counterpart): 256
+   * (blocks of 128 threads) or 128 (blocks of 64 threads; fewer idle warps on
+   * leaves and proxy sets that fill a 256-target tile only partly); 0: 256. */
+  int tile_targets;
 } btk_plan_desc;
 
 enum { BTK_DEGREE_FIXED = 0, BTK_DEGREE_PER_PAIR = 1 };
