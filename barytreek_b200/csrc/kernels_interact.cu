@@ -339,23 +339,29 @@ __device__ __forceinline__ void two_sum_add(double& sum, double& comp, double b)
   comp += e;
 }
 
-template <int DIM, int KIND, int THREADS>
-__global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 / THREADS)
-    k_interact_mixed(InteractParams p) {
+// Blocks per SM: potential + gradient and the vector kernel 4 * 128 /
+// THREADS (128 registers); the potential alone, at 128 threads, 6 with a
+// 2-stage ring (80 registers, 30.8 KB of shared memory; measured 299 -> 289 ms
+// on the 256-problem batch against 5 blocks with 3 stages), else 5 * 128 /
+// THREADS.
+template <int DIM, int KIND, int THREADS,
+          int STAGES = (KIND == BTK_KIND_POT && THREADS == 128) ? 2 : kStages,
+          int MINB = KIND == BTK_KIND_POT ? (THREADS == 128 ? 6 : 10) : 4 * 128 / THREADS>
+__global__ void __launch_bounds__(THREADS, MINB) k_interact_mixed(InteractParams p) {
   constexpr int NC = KernelTraits<DIM, KIND>::NC;
   constexpr int TPT = kTargetsPerThread;
   static_assert(TPT == 2, "targets of a warp are [64 w, 64 w + 64): two per thread");
   constexpr int kChunk = 2 * THREADS;  // sources per chunk: one pair per thread
   constexpr int kPairs = THREADS;
   constexpr int kFoldPairs = kPairs;
-  __shared__ __align__(128) double4 sbuf[kStages][kChunk];
+  __shared__ __align__(128) double4 sbuf[STAGES][kChunk];
   // converted chunk, by source pair j = (2j, 2j+1): negated hi coordinates and
   // weights, negated lo coordinates
   // (double-buffered: chunk c is converted into buffer c & 1 while other warps
   // may still evaluate chunk c - 1 from the other buffer)
   __shared__ __align__(16) float4 fA[2][kPairs], fB[2][kPairs], fL[2][kPairs];
   __shared__ __align__(16) float2 fLz[2][kPairs];
-  __shared__ __align__(8) uint64_t bars[kStages];
+  __shared__ __align__(8) uint64_t bars[STAGES];
   __shared__ int s_item, s_abort;
   __shared__ uint32_t s_fail_chunk;
   __shared__ int s_ncp[2][THREADS / 32];  // per warp region: pairs on the hi/lo path
@@ -363,7 +369,7 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5, tbase = warp * 64;
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
     s_abort = 0;
   }
@@ -387,7 +393,7 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
     const float thr = fmaxf(w.hx, fmaxf(w.hy, w.hz));  // near sources at least this far from the box: FP32 path
 
     auto issue = [&](int c) {
-      const int stage = (g + c) % kStages;
+      const int stage = (g + c) % STAGES;
       const int need = min(kChunk, w.s_total - c * kChunk);
       mbar_arrive_expect_tx(&bars[stage], (uint32_t)need * sizeof(double4));
       int filled = 0;
@@ -407,7 +413,7 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
     if (tid == 0) {
       pe = w.e_begin;
       poff = 0;
-      for (int c = 0; c < min(kStages, n_chunks); ++c) issue(c);
+      for (int c = 0; c < min(STAGES, n_chunks); ++c) issue(c);
     }
 
     // This warp's targets: [tbase, tbase + 64) of the tile, nu of its two
@@ -420,7 +426,7 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
       // (src/direct_sum_impl.hpp:34-94): absolute coordinates, the FP64
       // reciprocal square root, FP64 sums. Sources are read from the FP64
       // stage itself, so a stage is refilled only after the next chunk's
-      // barrier (every thread has finished it): chunk c - 1 + kStages is
+      // barrier (every thread has finished it): chunk c - 1 + STAGES is
       // issued at chunk c, one barrier per chunk.
       double ax[TPT], ay[TPT], az[TPT], a64[TPT][NC];
 #pragma unroll
@@ -433,8 +439,8 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
         for (int c = 0; c < NC; ++c) a64[u][c] = 0.0;
       }
       for (int c = 0; c < n_chunks; ++c) {
-        const int stage = (g + c) % kStages;
-        const uint32_t parity = ((g + c) / kStages) & 1u;
+        const int stage = (g + c) % STAGES;
+        const uint32_t parity = ((g + c) / STAGES) & 1u;
         if (!mbar_wait_bounded(&bars[stage], parity, p.wait_limit)) {
           s_abort = 1;
           s_fail_chunk = g + c;
@@ -442,7 +448,7 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
         }
         __syncthreads();
         if (s_abort) break;
-        if (tid == 0 && c >= 1 && c - 1 + kStages < n_chunks) issue(c - 1 + kStages);
+        if (tid == 0 && c >= 1 && c - 1 + STAGES < n_chunks) issue(c - 1 + STAGES);
         const int cnt = min(kChunk, w.s_total - c * kChunk);
         const double4* sb = sbuf[stage];
         if (p.eps2 < 1.1754943508222875e-38) {  // r^2 may leave the FP32 normal range: guarded
@@ -495,8 +501,8 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
     }
 
     for (int c = 0; c < n_chunks; ++c) {
-      const int stage = (g + c) % kStages;
-      const uint32_t parity = ((g + c) / kStages) & 1u;
+      const int stage = (g + c) % STAGES;
+      const uint32_t parity = ((g + c) / STAGES) & 1u;
       if (!mbar_wait_bounded(&bars[stage], parity, p.wait_limit)) {
         s_abort = 1;
         s_fail_chunk = g + c;
@@ -519,12 +525,23 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
           const int j = 2 * tid + k;
           if (j < cnt) {
             const double4 s = sbuf[stage][j];
-            split_rel(s.x, w.cx, hx[k], lx[k]);
-            split_rel(s.y, w.cy, hy[k], ly[k]);
-            split_rel(s.z, w.cz, hz[k], lz[k]);
+            const double rx = s.x - w.cx, ry = s.y - w.cy, rz = s.z - w.cz;
+            hx[k] = (float)rx;
+            hy[k] = (float)ry;
+            hz[k] = (float)rz;
             const float gap = fmaxf(fabsf(hx[k]) - w.hx,
                                     fmaxf(fabsf(hy[k]) - w.hy, DIM == 3 ? fabsf(hz[k]) - w.hz : -3.0e38f));
             close[k] = j < near_end && gap < thr;
+            // Low parts only where the hi/lo path reads them (close sources;
+            // a farther source sharing a hi/lo pair reads 0: its FP32 value);
+            // the FP64 <-> FP32 conversions share the MUFU pipe.
+            if (close[k]) {
+              lx[k] = (float)(rx - (double)hx[k]);
+              ly[k] = (float)(ry - (double)hy[k]);
+              lz[k] = (float)(rz - (double)hz[k]);
+            } else {
+              lx[k] = ly[k] = lz[k] = 0.f;
+            }
             hx[k] = -hx[k];
             hy[k] = -hy[k];
             hz[k] = -hz[k];
@@ -576,7 +593,7 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
       // stage has been read, so it is refilled while this chunk is evaluated.
       __syncthreads();
       if (s_abort) break;
-      if (tid == 0 && c + kStages < n_chunks) issue(c + kStages);
+      if (tid == 0 && c + STAGES < n_chunks) issue(c + STAGES);
       if (!split) {
         const int np = (cnt + 1) / 2, nnp = (near_end + 1) / 2;  // a pair with one near source is near
         for (int f0 = 0; f0 < np; f0 += kFoldPairs) {
@@ -652,7 +669,7 @@ __global__ void __launch_bounds__(THREADS, (KIND == BTK_KIND_POT ? 5 : 4) * 128 
   }
   if (s_abort && tid == 0) {
     for (uint32_t k = s_fail_chunk; k < issued; ++k)
-      mbar_wait_bounded(&bars[k % kStages], (k / kStages) & 1u, kDrainLimit);
+      mbar_wait_bounded(&bars[k % STAGES], (k / STAGES) & 1u, kDrainLimit);
   }
 }
 

@@ -285,8 +285,9 @@ def event_ms(fn, flush):
 # DRAM bytes (read + write) of one launch of the headline form's interaction
 # kernel at the full workload, from one ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum; profiles/k_interact_mixed_learned_1m_traffic.md gives
-# the command). None when the workload differs from the captured one.
-TRAFFIC_BYTES = {}
+# the command and the algorithmic bytes it compares with). None when the
+# workload differs from the captured one.
+TRAFFIC_BYTES = {("k_interact_mixed", "learned", 2, 1 << 20): 1730000000 + 192830000}
 
 
 class Form:
