@@ -87,7 +87,7 @@ class Forest(ctypes.Structure):
 
 class BatchDesc(ctypes.Structure):
     _fields_ = [("forest", ForestDesc), ("kind", ctypes.c_int), ("precision", ctypes.c_int),
-                ("work_split", ctypes.c_int)]
+                ("work_split", ctypes.c_int), ("tile_targets", ctypes.c_int)]
 
 
 class BatchStats(ctypes.Structure):

@@ -54,7 +54,7 @@ class Batch:
     """
 
     def __init__(self, coords_list, *, degree=6, theta=0.6, eps=1e-4, kind=KIND_POT, precision=PREC_MIXED,
-                 cluster_size=None, table=None, work_split=None, device="cuda"):
+                 cluster_size=None, table=None, work_split=None, tile_targets=None, device="cuda"):
         import torch
 
         self.dim = len(coords_list[0])
@@ -67,10 +67,13 @@ class Batch:
             cluster_size = [table.leaf_for(int(n)) for n in self.sizes]
             if work_split is None:
                 work_split = table.split_for_batch(self.sizes)
+            if tile_targets is None:
+                tile_targets = table.tile_for_batch(self.sizes)
         if np.isscalar(cluster_size):
             cluster_size = [int(cluster_size)] * len(coords_list)
         self.cluster_size = np.ascontiguousarray(cluster_size, np.int32)
         self.work_split = int(work_split or 0)
+        self.tile_targets = int(tile_targets or 0)
         self.kind, self.precision = kind, precision
         self.ncomp = 1 if kind == KIND_POT else (3 if kind == _lib.KIND_VEL else 1 + self.dim)
         xyz = [np.ascontiguousarray(np.concatenate([c[d] for c in coords_list]), np.float64) for d in range(self.dim)]
@@ -80,6 +83,7 @@ class Batch:
         d.forest.point_offset = ptr(self.offsets)
         d.forest.cluster_size = ptr(self.cluster_size)
         d.kind, d.precision, d.work_split = kind, precision, self.work_split
+        d.tile_targets = self.tile_targets
         self.device = torch.device(device)
         self._h = ctypes.c_void_p()
         stream = torch.cuda.current_stream(self.device).cuda_stream
@@ -126,13 +130,16 @@ class Batch:
 
 
 class Autotuner:
-    """Per-bucket leaf size and work split, chosen by timing batched solves."""
+    """Per-bucket leaf size, work split and tile size (targets per work item),
+    chosen by timing batched solves."""
 
-    LEAVES = (128, 256, 512, 1024, 2048)
+    LEAVES = (128, 256, 512, 1024, 2048, 4096)
     SPLITS = (4, 8, 16)
+    TILES = (256, 128)
 
     def __init__(self, table: dict | None = None, meta: dict | None = None):
-        self.table = {int(k): tuple(v) for k, v in (table or {}).items()}  # bucket -> (leaf, split)
+        # bucket -> (leaf, split[, tile]); tables without a tile mean 256
+        self.table = {int(k): tuple(v) for k, v in (table or {}).items()}
         self.meta = meta or {}
 
     # -- persistence
@@ -155,22 +162,29 @@ class Autotuner:
         near = min(self.table, key=lambda k: abs(k - b))
         return self.table[near][0]
 
-    def split_for_batch(self, sizes) -> int:
-        """The work split of the bucket holding most of the batch's points."""
+    def _main_bucket(self, sizes) -> int:
         w = {}
         for n in sizes:
             b = bucket_of(int(n))
             w[b] = w.get(b, 0) + int(n)
-        b = max(w, key=w.get)
-        return self.table.get(b, (0, 8))[1]
+        return max(w, key=w.get)
+
+    def split_for_batch(self, sizes) -> int:
+        """The work split of the bucket holding most of the batch's points."""
+        return self.table.get(self._main_bucket(sizes), (0, 8))[1]
+
+    def tile_for_batch(self, sizes) -> int:
+        """The tile size of the bucket holding most of the batch's points."""
+        e = self.table.get(self._main_bucket(sizes), (0, 8))
+        return e[2] if len(e) > 2 else 256
 
     # -- tuning
     @staticmethod
-    def _time_batch(coords, q, leaf, split, degree, theta, eps, kind, precision, reps):
+    def _time_batch(coords, q, leaf, split, degree, theta, eps, kind, precision, reps, tile=256):
         import torch
 
         b = Batch(coords, degree=degree, theta=theta, eps=eps, kind=kind, precision=precision, cluster_size=leaf,
-                  work_split=split)
+                  work_split=split, tile_targets=tile)
         qd = torch.from_numpy(q).cuda()
         out = torch.empty((b.ncomp, b.n), dtype=torch.float64, device="cuda")
         b.solve(qd, out)  # capture
@@ -183,11 +197,14 @@ class Autotuner:
         return float(np.median(ts))
 
     def tune(self, buckets=range(12, 18), *, points_per_batch=1 << 20, degree=6, theta=0.6, eps=1e-4,
-             kind=KIND_POT, precision=PREC_MIXED, leaves=None, splits=None, reps=3, seed=900, log=None):
-        """Times every leaf size (at split 8), then every split at the best
-        leaf, on a mini-batch of representative problems per bucket."""
+             kind=KIND_POT, precision=PREC_MIXED, leaves=None, splits=None, tiles=None, reps=3, seed=900,
+             log=None):
+        """Times every leaf size (at split 8, tile 256), then every split at
+        the best leaf, then every tile size at the best pair, on a mini-batch
+        of representative problems per bucket."""
         leaves = tuple(leaves or self.LEAVES)
         splits = tuple(splits or self.SPLITS)
+        tiles = tuple(tiles or self.TILES)
         times = {}
         for k in buckets:
             n = int(round(2.0 ** (k + 0.5)))
@@ -203,11 +220,17 @@ class Autotuner:
                 if sp not in ts:
                     ts[sp] = self._time_batch(coords, q, best_leaf, sp, degree, theta, eps, kind, precision, reps)
             best_split = min(ts, key=ts.get)
-            self.table[k] = (best_leaf, best_split)
-            times[k] = {"n": n, "problems": count, "leaf_ms": tl, "split_ms": ts}
+            tt = {256: ts[best_split]}
+            for tile in tiles:
+                if tile not in tt:
+                    tt[tile] = self._time_batch(coords, q, best_leaf, best_split, degree, theta, eps, kind, precision,
+                                                reps, tile)
+            best_tile = min(tt, key=tt.get)
+            self.table[k] = (best_leaf, best_split, best_tile)
+            times[k] = {"n": n, "problems": count, "leaf_ms": tl, "split_ms": ts, "tile_ms": tt}
             if log:
-                log(f"bucket 2^{k}: n={n} x{count}: leaf {best_leaf} split {best_split} "
-                    f"({ts[best_split]:.2f} ms; leaves {', '.join(f'{a}:{b:.2f}' for a, b in tl.items())})")
+                log(f"bucket 2^{k}: n={n} x{count}: leaf {best_leaf} split {best_split} tile {best_tile} "
+                    f"({tt[best_tile]:.2f} ms; leaves {', '.join(f'{a}:{b:.2f}' for a, b in tl.items())})")
         self.meta = {"degree": degree, "theta": theta, "eps": eps, "kind": kind, "precision": precision,
                      "points_per_batch": points_per_batch, "times_ms": {str(k): v for k, v in times.items()}}
         return self

@@ -336,6 +336,7 @@ btk_status btk_batch_create(btk_batch** out, const btk_batch_desc* desc, const d
   pd.precision = desc->precision;
   pd.degree_mode = BTK_DEGREE_FIXED;
   pd.work_split = desc->work_split;
+  pd.tile_targets = desc->tile_targets;
   s = btk_plan_create(&b->plan, &pd, stream);
   if (s != BTK_OK) return fail(s);
   const size_t n = (size_t)std::max<int64_t>(b->n_points, 1);

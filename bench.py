@@ -800,7 +800,8 @@ def run_batch(args, flush):
         "graph_launches_per_step": 1, "kernel_launches_per_step": launches, "work_items": st["work_items"],
         "levels": st["levels"], "panels": st["panel_count"], "setup_s": setup,
         "leaf_size_by_bucket": {f"2^{k}": v[0] for k, v in sorted(table.table.items())},
-        "work_split": b.work_split, "rel_l2_vs_direct_sampled": (err2 / ref2) ** 0.5 if ref2 > 0 else None,
+        "work_split": b.work_split, "tile_targets": b.tile_targets or 256,
+        "rel_l2_vs_direct_sampled": (err2 / ref2) ** 0.5 if ref2 > 0 else None,
         "clocks": clk.summary(),
     }
     b.close()

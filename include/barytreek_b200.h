@@ -617,6 +617,7 @@ typedef struct {
   int kind;       /* btk_kind */
   int precision;  /* btk_precision */
   int work_split; /* work items per persistent-grid slot (0 = 8) */
+  int tile_targets; /* targets per interaction work item: 256 or 128 (0 = 256) */
 } btk_batch_desc;
 
 /* Builds the forest and its plan and uploads the coordinates (HOST arrays,
