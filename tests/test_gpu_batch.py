@@ -84,6 +84,7 @@ def test_autotuner_picks_per_bucket():
     from barytreek_b200.batch import Autotuner
     t = Autotuner().tune(buckets=[12, 14], points_per_batch=1 << 16, leaves=(128, 512), splits=(4, 8), reps=1)
     for k in (12, 14):
-        leaf, split = t.table[k]
-        assert leaf in (128, 512) and split in (4, 8)
+        leaf, split, tile = t.table[k]
+        assert leaf in (128, 512) and split in (4, 8) and tile in (128, 256)
     assert t.leaf_for(5000) == t.table[12][0]
+    assert t.tile_for_batch([5000, 5000, 20000]) == t.table[12][2]
