@@ -108,3 +108,15 @@ def test_forest_rejects_bad_descriptors(lib):
     d = _lib.ForestDesc(3, 13, 0.6, 1e-4, 1, None, None)
     assert lib.btk_forest_build(ctypes.byref(d), None, None, None, ctypes.byref(_lib.Forest())) == \
         _lib.ERR_UNSUPPORTED
+
+
+def test_autotuner_table_lookup():
+    """Per-bucket lookup of the autotuner's table: leaf size by problem size,
+    work split and tile size from the bucket holding most of a batch's points;
+    two-entry tables (no tile) mean tiles of 256."""
+    from barytreek_b200.batch import Autotuner
+    t = Autotuner({12: (1024, 16, 256), 14: (512, 8, 128)})
+    assert t.leaf_for(5000) == 1024 and t.leaf_for(20000) == 512 and t.leaf_for(9000) == 1024
+    assert t.split_for_batch([5000] * 5 + [20000]) == 16 and t.tile_for_batch([5000] * 5 + [20000]) == 256
+    assert t.split_for_batch([5000, 5000, 20000]) == 8 and t.tile_for_batch([5000, 5000, 20000]) == 128
+    assert Autotuner({12: (1024, 16)}).tile_for_batch([5000]) == 256

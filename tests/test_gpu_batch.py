@@ -87,4 +87,4 @@ def test_autotuner_picks_per_bucket():
         leaf, split, tile = t.table[k]
         assert leaf in (128, 512) and split in (4, 8) and tile in (128, 256)
     assert t.leaf_for(5000) == t.table[12][0]
-    assert t.tile_for_batch([5000, 5000, 20000]) == t.table[12][2]
+    assert t.tile_for_batch([5000] * 5 + [20000]) == t.table[12][2]  # bucket 2^12 holds most points
