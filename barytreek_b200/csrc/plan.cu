@@ -2074,7 +2074,10 @@ struct DropinEntry {
 };
 
 std::mutex g_dropin_mu;
-std::vector<std::unique_ptr<DropinEntry>> g_dropin;  // at most kDropinEntries
+// At most kDropinEntries. Held on the heap and never destroyed, so no CUDA
+// call runs from a static destructor at process exit (the runtime may be shut
+// down by then); btk_dropin_cache_clear frees the entries.
+std::vector<std::unique_ptr<DropinEntry>>& g_dropin = *new std::vector<std::unique_ptr<DropinEntry>>();
 uint64_t g_dropin_clock = 0;
 constexpr size_t kDropinEntries = 6;
 
