@@ -193,7 +193,7 @@ cudaError_t launch_pair_features(int n_pairs, const int* ptype, const int* ptgt,
                                  const DevPanel* ps, double root_radius, double eps, const float* desc_s,
                                  int n_points, const double4* pts, double* gsum, float* feat, cudaStream_t s);
 cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const float* feat, float* out,
-                             cudaStream_t s);
+                             int* status, cudaStream_t s);  // status: optional device word, set on a timeout
 // Pairs [conv0, n_pc) of the PC block are leaf pairs that may stay direct
 // (degree 0); pc_direct[2 i], [2 i + 1]: their source leaf's first point and
 // point count.

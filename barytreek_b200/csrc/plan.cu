@@ -1571,7 +1571,7 @@ btk_status btk_selector_predict(const btk_selector* s, int n, const float* featu
                                 btk_stream_t stream) {
   BTK_CHECK(s && n >= 0 && (n == 0 || (features && out)), BTK_ERR_INVALID_ARGUMENT,
             "btk_selector_predict: bad argument");
-  BTK_CUDA(launch_mlp_infer(n, s->d_w, s->norm, features, out, (cudaStream_t)stream));
+  BTK_CUDA(launch_mlp_infer(n, s->d_w, s->norm, features, out, nullptr, (cudaStream_t)stream));
   return BTK_OK;
 }
 
@@ -1621,7 +1621,7 @@ btk_status btk_plan_execute_learned(btk_plan* P, const btk_selector* sel, double
   P->deg_learned = true;
   // Upward pass and features, then the selector's degrees.
   BTK_TRY(btk_plan_pair_features(P, xs, ys, zs, charges, P->d_feat, stream));
-  BTK_CUDA(launch_mlp_infer(P->n_pairs, sel->d_w, sel->norm, P->d_feat, P->d_pred, st));
+  BTK_CUDA(launch_mlp_infer(P->n_pairs, sel->d_w, sel->norm, P->d_feat, P->d_pred, P->d_ticket_status + 1, st));
   const int lo = std::max(std::max(degree_lo, P->degree_min), 1);
   if (P->degree_rule == BTK_DEGREE_RULE_COST)
     BTK_CUDA(launch_choose_degrees_cost(P->n_pairs, P->dim, P->n_pc, P->n_cp, P->n_pc_list, P->d_pred,

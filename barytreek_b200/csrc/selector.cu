@@ -10,6 +10,8 @@
 // chosen on the device. Training uses error samples generated here: each
 // sampled pair is evaluated at every degree through its proxies and compared
 // with the direct sum over the source cluster's points, in FP64.
+#include <atomic>
+
 #include "device_math.cuh"
 #include "kernels.cuh"
 
@@ -206,134 +208,177 @@ __device__ __forceinline__ void mlp_row(const float* sw, const float* x, float* 
 }
 
 // Inference on raw features, out[i][o] = predicted log10 error at degree 4+o,
-// on the tensor cores: each warp pushes 16 pairs through the three layers as
-// mma.sync m16n8k16 BF16 products with FP32 accumulation (layer 1: 8 column
-// tiles of K = 16; layer 2: 8 x 4 of K = 64; layer 3: 2 column tiles, outputs
-// 9..15 zero). The accumulator layout of one layer (rows g and g + 8, columns
-// 2t, 2t + 1 of each 8-column tile, g = lane / 4, t = lane % 4) is the A
-// operand layout of the next layer's K = 16 steps, so activations stay in
-// registers: bias, ReLU and the round to BF16 are applied in place. Weights
-// sit in shared memory as BF16 rows padded to 24 / 72 elements, which puts the
-// 32 lanes' B-operand words in 32 different banks. Normalised inputs and
-// hidden activations are rounded to BF16 (the training kernels keep them in
-// FP32; the difference is within the network's error).
-constexpr int kW1Row = kF + 8, kW2Row = kH + 8;  // padded BF16 row lengths
-struct InferSmem {
-  __nv_bfloat16 w1[kH * kW1Row], w2[kH * kW2Row], w3[16 * kW2Row];
+// on the 5th-generation tensor cores (tcgen05, kind::f16: BF16 operands, FP32
+// accumulators in TMEM). A CTA of 128 threads owns tiles of 128 pairs (the MMA
+// M; thread t's pair is TMEM lane t) and pushes each through the three layers:
+//   layer 1: A = normalised features [128 x 16], B = W1 [64 x 16]  -> D1 [128 x 64]
+//   layer 2: A = ReLU(D1 + b1) [128 x 64], B = W2 [64 x 64] (4 K steps) -> D2
+//   layer 3: A = ReLU(D2 + b2), B = W3 [9 (padded to 16) x 64] -> D3 [128 x 16]
+// One thread issues each layer's MMAs and commits them to an mbarrier; every
+// thread then reads its lane's accumulators with tcgen05.ld, applies bias,
+// ReLU and the BF16 rounding, and writes its row of the next layer's A tile
+// (K-major, no swizzle). The weights are staged once per CTA. Normalised
+// inputs and hidden activations are BF16 (the training kernels keep them in
+// FP32; the difference is within the network's error). Waits are bounded: a
+// CTA that gives up sets *status (when given), stops and frees its TMEM.
+constexpr int kTcM = 128;          // pairs per tile (MMA M), one per thread
+constexpr uint32_t kTmemCols = 128;  // D1/D2 in columns 0..63, D3 in 64..79
+constexpr uint32_t kTcWaitLimit = 1u << 22;
+struct TcSmem {
+  alignas(1024) uint8_t a1[kTcM * kF * 2];  // layer-1 A, K = 16
+  alignas(1024) uint8_t a2[kTcM * kH * 2];  // layer-2, then layer-3 A, K = 64 (4 K steps of 4096 B)
+  alignas(1024) uint8_t w1[kH * kF * 2];    // N = 64, K = 16
+  alignas(1024) uint8_t w2[kH * kH * 2];    // N = 64, K = 64 (4 K steps of 2048 B)
+  alignas(1024) uint8_t w3[16 * kH * 2];    // N = 16, K = 64 (4 K steps of 512 B); rows 9..15 zero
   float b1[kH], b2[kH], b3[16];
+  uint64_t bar;
+  uint32_t tmem;
+  int abort;
 };
+// At least this much dynamic shared memory per CTA, so at most 3 CTAs share an
+// SM and their TMEM columns (3 x 128 <= 512) never run out.
+constexpr size_t kTcSmemBytes = 64 * 1024;
+static_assert(sizeof(TcSmem) + 1024 <= kTcSmemBytes, "tile buffers exceed the reserved shared memory");
+
+// Byte offset of BF16 element (row, k) in a K-major, unswizzled tile of R rows:
+// K steps of 16 elements are R x 32 bytes apart; within one, 8-row groups are
+// 256 bytes apart (sbo) and the two 8-element halves 128 bytes apart (lbo).
+__device__ __forceinline__ uint32_t kmaj_off(int row, int k, int R) {
+  return (uint32_t)((k >> 4) * (R * 32) + (row >> 3) * 256 + ((k >> 3) & 1) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-__device__ __forceinline__ void mma_bf16(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                         uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-      "{%0, %1, %2, %3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+// 16 values of row `row` (columns k0..k0+15) into a K-major tile as BF16.
+__device__ __forceinline__ void store_row16(uint8_t* tile, int row, int k0, int R, const float* v) {
+  uint4 lo, hi;
+  lo.x = pack_bf16x2(v[0], v[1]);
+  lo.y = pack_bf16x2(v[2], v[3]);
+  lo.z = pack_bf16x2(v[4], v[5]);
+  lo.w = pack_bf16x2(v[6], v[7]);
+  hi.x = pack_bf16x2(v[8], v[9]);
+  hi.y = pack_bf16x2(v[10], v[11]);
+  hi.z = pack_bf16x2(v[12], v[13]);
+  hi.w = pack_bf16x2(v[14], v[15]);
+  *reinterpret_cast<uint4*>(tile + kmaj_off(row, k0, R)) = lo;
+  *reinterpret_cast<uint4*>(tile + kmaj_off(row, k0 + 8, R)) = hi;
 }
 
-__global__ void __launch_bounds__(128) k_mlp_infer(int n, const __nv_bfloat16* w, MlpNorm nrm, const float* feat,
-                                                   float* out) {
-  __shared__ __align__(16) InferSmem sm;
-  for (int o = threadIdx.x; o < kH * kW1Row; o += blockDim.x) {
-    const int r = o / kW1Row, c = o % kW1Row;
-    sm.w1[o] = c < kF ? w[kW1 + r * kF + c] : __float2bfloat16(0.f);
-  }
-  for (int o = threadIdx.x; o < kH * kW2Row; o += blockDim.x) {
-    const int r = o / kW2Row, c = o % kW2Row;
-    sm.w2[o] = c < kH ? w[kW2 + r * kH + c] : __float2bfloat16(0.f);
-  }
-  for (int o = threadIdx.x; o < 16 * kW2Row; o += blockDim.x) {
-    const int r = o / kW2Row, c = o % kW2Row;
-    sm.w3[o] = (r < kO && c < kH) ? w[kW3 + r * kH + c] : __float2bfloat16(0.f);
-  }
-  for (int o = threadIdx.x; o < kH; o += blockDim.x) {
+__global__ void __launch_bounds__(kTcM) k_mlp_infer(int n, const __nv_bfloat16* w, MlpNorm nrm, const float* feat,
+                                                   float* out, int* status) {
+  extern __shared__ uint8_t dsm_raw[];
+  TcSmem& sm = *reinterpret_cast<TcSmem*>(dsm_raw + ((1024u - (smem_addr(dsm_raw) & 1023u)) & 1023u));
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int o = tid; o < kH * kF; o += kTcM)
+    *reinterpret_cast<__nv_bfloat16*>(sm.w1 + kmaj_off(o / kF, o % kF, kH)) = w[kW1 + o];
+  for (int o = tid; o < kH * kH; o += kTcM)
+    *reinterpret_cast<__nv_bfloat16*>(sm.w2 + kmaj_off(o / kH, o % kH, kH)) = w[kW2 + o];
+  for (int o = tid; o < 16 * kH; o += kTcM)
+    *reinterpret_cast<__nv_bfloat16*>(sm.w3 + kmaj_off(o / kH, o % kH, 16)) =
+        o / kH < kO ? w[kW3 + o] : __float2bfloat16(0.f);
+  for (int o = tid; o < kH; o += kTcM) {
     sm.b1[o] = __bfloat162float(w[kB1 + o]);
     sm.b2[o] = __bfloat162float(w[kB2 + o]);
   }
-  if (threadIdx.x < 16) sm.b3[threadIdx.x] = threadIdx.x < kO ? __bfloat162float(w[kB3 + threadIdx.x]) : 0.f;
+  if (tid < 16) sm.b3[tid] = tid < kO ? __bfloat162float(w[kB3 + tid]) : 0.f;
+  if (tid == 0) {
+    mbar_init(&sm.bar, 1);
+    mbar_fence_init();
+    sm.abort = 0;
+  }
+  if (warp == 0) {
+    tmem_alloc(&sm.tmem, kTmemCols);
+    tmem_relinquish();
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
   __syncthreads();
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int warps = gridDim.x * (blockDim.x >> 5);
-  for (int tile = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 16 < n; tile += warps) {
-    const int r0 = tile * 16 + g, r1 = r0 + 8;  // this lane's two pairs
-    // layer 1 A operand: normalised features, columns 2t, 2t + 1 and 2t + 8, 2t + 9
-    float x[2][4];
+  tc_fence_after();
+  const uint32_t tbase = sm.tmem;
+  const uint32_t taddr = tbase + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
+  constexpr uint32_t id64 = umma_idesc_bf16_f32(kTcM, kH), id16 = umma_idesc_bf16_f32(kTcM, 16);
+  uint32_t phase = 0, issued = 0, waited = 0;
+  // Waits for the MMAs committed last; false (and the CTA stops) on timeout.
+  auto wait_mma = [&]() {
+    if (mbar_wait_bounded(&sm.bar, phase, kTcWaitLimit)) {
+      phase ^= 1u;
+      ++waited;
+    } else {  // still in flight: the drain below waits for it
+      sm.abort = 1;
+      if (status) atomicCAS(status, 0, (int)BTK_ERR_DEVICE_TIMEOUT);
+    }
+    __syncthreads();
+    tc_fence_after();
+    return sm.abort == 0;
+  };
+  const int tiles = (n + kTcM - 1) / kTcM;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int row = tile * kTcM + tid;
+    {  // layer-1 A: this thread's normalised features
+      float x[kF];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = h ? r1 : r0;
+      for (int c = 0; c < kF; ++c) x[c] = row < n ? (feat[(size_t)row * kF + c] - nrm.xm[c]) / nrm.xs[c] : 0.f;
+      store_row16(sm.a1, tid, 0, kTcM, x);
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      umma_bf16(tbase, umma_desc_kmajor(sm.a1, 128, 256), umma_desc_kmajor(sm.w1, 128, 256), id64, 0);
+      umma_commit(&sm.bar);
+      ++issued;
+    }
+    if (!wait_mma()) break;
+#pragma unroll 1
+    for (int layer = 0; layer < 2; ++layer) {  // D1 -> layer-2 A, D2 -> layer-3 A
+      const float* bias = layer == 0 ? sm.b1 : sm.b2;
+#pragma unroll 1
+      for (int c0 = 0; c0 < kH; c0 += 16) {
+        float v[16];
+        tmem_ld16(taddr + (uint32_t)c0, v);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int c = 2 * t + (q & 1) + (q >> 1) * 8;
-        x[h][q] = r < n ? (feat[(size_t)r * kF + c] - nrm.xm[c]) / nrm.xs[c] : 0.f;
+        for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k] + bias[c0 + k], 0.f);
+        store_row16(sm.a2, tid, c0, kTcM, v);
       }
-    }
-    const uint32_t a10 = pack_bf16x2(x[0][0], x[0][1]), a11 = pack_bf16x2(x[1][0], x[1][1]);
-    const uint32_t a12 = pack_bf16x2(x[0][2], x[0][3]), a13 = pack_bf16x2(x[1][2], x[1][3]);
-    float h1[8][4];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const __nv_bfloat16* wr = sm.w1 + (8 * j + g) * kW1Row + 2 * t;
-      h1[j][0] = h1[j][1] = h1[j][2] = h1[j][3] = 0.f;
-      mma_bf16(h1[j], a10, a11, a12, a13, *reinterpret_cast<const uint32_t*>(wr),
-               *reinterpret_cast<const uint32_t*>(wr + 8));
-      const int c = 8 * j + 2 * t;
-      h1[j][0] = fmaxf(h1[j][0] + sm.b1[c], 0.f);
-      h1[j][1] = fmaxf(h1[j][1] + sm.b1[c + 1], 0.f);
-      h1[j][2] = fmaxf(h1[j][2] + sm.b1[c], 0.f);
-      h1[j][3] = fmaxf(h1[j][3] + sm.b1[c + 1], 0.f);
-    }
-    uint32_t a2[4][4];
-#pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
-      a2[kk][0] = pack_bf16x2(h1[2 * kk][0], h1[2 * kk][1]);
-      a2[kk][1] = pack_bf16x2(h1[2 * kk][2], h1[2 * kk][3]);
-      a2[kk][2] = pack_bf16x2(h1[2 * kk + 1][0], h1[2 * kk + 1][1]);
-      a2[kk][3] = pack_bf16x2(h1[2 * kk + 1][2], h1[2 * kk + 1][3]);
-    }
-    float h2[8][4];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      h2[j][0] = h2[j][1] = h2[j][2] = h2[j][3] = 0.f;
-#pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        const __nv_bfloat16* wr = sm.w2 + (8 * j + g) * kW2Row + 16 * kk + 2 * t;
-        mma_bf16(h2[j], a2[kk][0], a2[kk][1], a2[kk][2], a2[kk][3], *reinterpret_cast<const uint32_t*>(wr),
-                 *reinterpret_cast<const uint32_t*>(wr + 8));
+      fence_proxy_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        for (int ks = 0; ks < kH / 16; ++ks) {
+          const uint64_t da = umma_desc_kmajor(sm.a2 + ks * (kTcM * 32), 128, 256);
+          if (layer == 0)
+            umma_bf16(tbase, da, umma_desc_kmajor(sm.w2 + ks * (kH * 32), 128, 256), id64, ks > 0);
+          else
+            umma_bf16(tbase + 64, da, umma_desc_kmajor(sm.w3 + ks * (16 * 32), 128, 256), id16, ks > 0);
+        }
+        umma_commit(&sm.bar);
+        ++issued;
       }
-      const int c = 8 * j + 2 * t;
-      h2[j][0] = fmaxf(h2[j][0] + sm.b2[c], 0.f);
-      h2[j][1] = fmaxf(h2[j][1] + sm.b2[c + 1], 0.f);
-      h2[j][2] = fmaxf(h2[j][2] + sm.b2[c], 0.f);
-      h2[j][3] = fmaxf(h2[j][3] + sm.b2[c + 1], 0.f);
+      if (!wait_mma()) break;
     }
+    if (sm.abort) break;
+    float v[16];
+    tmem_ld16(taddr + 64, v);
+    if (row < n) {
 #pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
-      a2[kk][0] = pack_bf16x2(h2[2 * kk][0], h2[2 * kk][1]);
-      a2[kk][1] = pack_bf16x2(h2[2 * kk][2], h2[2 * kk][3]);
-      a2[kk][2] = pack_bf16x2(h2[2 * kk + 1][0], h2[2 * kk + 1][1]);
-      a2[kk][3] = pack_bf16x2(h2[2 * kk + 1][2], h2[2 * kk + 1][3]);
+      for (int o = 0; o < kO; ++o) out[(size_t)row * kO + o] = (v[o] + sm.b3[o]) * nrm.ys + nrm.ym;
     }
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      float y[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        const __nv_bfloat16* wr = sm.w3 + (8 * j + g) * kW2Row + 16 * kk + 2 * t;
-        mma_bf16(y, a2[kk][0], a2[kk][1], a2[kk][2], a2[kk][3], *reinterpret_cast<const uint32_t*>(wr),
-                 *reinterpret_cast<const uint32_t*>(wr + 8));
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int c = 8 * j + 2 * t + (q & 1), r = (q >> 1) ? r1 : r0;
-        if (c < kO && r < n) out[(size_t)r * kO + c] = (y[q] + sm.b3[c]) * nrm.ys + nrm.ym;
-      }
-    }
+    tc_fence_before();
+    __syncthreads();  // every lane's TMEM reads are done before the next tile's MMAs
+    tc_fence_after();
+  }
+  // After a timeout, wait (bounded) for what thread 0 still has in flight
+  // before the TMEM columns are released.
+  if (tid == 0)
+    for (; waited < issued; ++waited, phase ^= 1u) mbar_wait_bounded(&sm.bar, phase, kTcWaitLimit);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tbase, kTmemCols);
   }
 }
 
@@ -915,7 +960,7 @@ cudaError_t launch_pair_features(int n_pairs, const int* ptype, const int* ptgt,
 }
 
 cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const float* feat, float* out,
-                             cudaStream_t s) {
+                             int* status, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   MlpNorm nrm;
   for (int k = 0; k < kF; ++k) {
@@ -924,14 +969,23 @@ cudaError_t launch_mlp_infer(int n, const void* w_bf16, const float* norm, const
   }
   nrm.ym = norm[2 * kF];
   nrm.ys = norm[2 * kF + 1] > 0 ? norm[2 * kF + 1] : 1.f;
-  // 16 pairs per warp, 4 warps per block; at most 8 blocks per SM's worth of
-  // blocks, each looping over its tiles (the weights are staged once per block)
+  // Tiles of 128 pairs; two CTAs per SM, each looping over its tiles (the
+  // weights are staged once per CTA). The shared-memory opt-in is set once
+  // per device.
   int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int tiles = (n + 15) / 16;
-  const int grid = std::max(1, std::min((tiles + 3) / 4, 8 * sms));
-  k_mlp_infer<<<grid, 128, 0, s>>>(n, (const __nv_bfloat16*)w_bf16, nrm, feat, out);
+  static std::atomic<uint64_t> opted{0};
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(opted.load(std::memory_order_acquire) & bit)) {
+    e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes);
+    if (e != cudaSuccess) return e;
+    opted.fetch_or(bit, std::memory_order_release);
+  }
+  const int tiles = (n + kTcM - 1) / kTcM;
+  const int grid = std::max(1, std::min(tiles, 2 * sms));
+  k_mlp_infer<<<grid, kTcM, kTcSmemBytes, s>>>(n, (const __nv_bfloat16*)w_bf16, nrm, feat, out, status);
   count_launch();
   return cudaGetLastError();
 }
