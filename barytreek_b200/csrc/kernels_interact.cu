@@ -15,7 +15,8 @@
 // mbarrier); all 128 threads evaluate their 2 targets against every source of a
 // chunk (broadcast shared-memory reads) and keep the sums in registers. One
 // block barrier per chunk. Warp w
-// owns targets [64 w, 64 w + 64) of a tile; warps whose targets lie past the
+// owns targets 32 w + lane and 32 w + THREADS + lane of a tile (a partly
+// filled tile spreads over all warps first); warps whose targets lie past the
 // tile's count skip the arithmetic. Each
 // target's sum is written once at the end of its item, so results need no
 // atomics unless the host split a long source list (kItemAtomic).
@@ -102,14 +103,14 @@ template <int DIM, int KIND, bool GUARD, int THREADS>
 __global__ void __launch_bounds__(THREADS, 768 / THREADS) k_interact_fp64(InteractParams p) {
   constexpr int NC = KernelTraits<DIM, KIND>::NC;
   constexpr int TPT = kTargetsPerThread;
-  static_assert(TPT == 2, "targets of a warp are [64 w, 64 w + 64): two per thread");
+  static_assert(TPT == 2, "targets of warp w are 32 w + lane and 32 w + THREADS + lane");
   __shared__ __align__(128) double4 sbuf[kStages][kChunk];
   __shared__ __align__(8) uint64_t bars[kStages];
   __shared__ int s_item, s_abort;
   __shared__ uint32_t s_fail_chunk;
 
   const int tid = threadIdx.x;
-  const int lane = tid & 31, tbase = (tid >> 5) * 64;
+  const int lane = tid & 31, tbase = (tid >> 5) * 32;
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
@@ -157,14 +158,16 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS) k_interact_fp64(Intera
       for (int c = 0; c < min(kStages, n_chunks); ++c) issue(c);
     }
 
-    // This warp's targets: [tbase, tbase + 64) of the tile, nu of its two
-    // 32-target halves in use (warp-uniform), so a partly filled tile leaves
-    // its idle warps' issue slots to other blocks.
-    const int nu = w.t_count > tbase + 32 ? 2 : (w.t_count > tbase ? 1 : 0);
+    // This warp's targets: [tbase, tbase + 32) and [tbase + THREADS, tbase +
+    // THREADS + 32) of the tile, nu of the two in use (warp-uniform). A tile
+    // of up to THREADS targets gives every warp up to 32 of them, so a partly
+    // filled tile keeps all of the block's warps busy: the warps of a block sit
+    // on different SM sub-partitions, whose MUFU and FMA pipes are separate.
+    const int nu = w.t_count > tbase + THREADS ? 2 : (w.t_count > tbase ? 1 : 0);
     double tx[TPT], ty[TPT], tz[TPT], acc[TPT][NC];
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int i = min(tbase + u * 32 + lane, w.t_count - 1);
+      const int i = min(tbase + u * THREADS + lane, w.t_count - 1);
       const double4 t = ((w.flags & kItemAudit) ? p.T4a : p.T4)[w.t_begin + i];
       tx[u] = t.x;
       ty[u] = t.y;
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS) k_interact_fp64(Intera
 
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int i = tbase + u * 32 + lane;
+      const int i = tbase + u * THREADS + lane;
       if (i < w.t_count) {
         const bool audit = (w.flags & kItemAudit) != 0;
         const int idx = audit ? w.t_begin + i : p.T_out[w.t_begin + i];
@@ -349,7 +352,7 @@ template <int DIM, int KIND, int THREADS, int STAGES = KIND == BTK_KIND_POT ? 2 
 __global__ void __launch_bounds__(THREADS, MINB) k_interact_mixed(InteractParams p) {
   constexpr int NC = KernelTraits<DIM, KIND>::NC;
   constexpr int TPT = kTargetsPerThread;
-  static_assert(TPT == 2, "targets of a warp are [64 w, 64 w + 64): two per thread");
+  static_assert(TPT == 2, "targets of warp w are 32 w + lane and 32 w + THREADS + lane");
   constexpr int kChunk = 2 * THREADS;  // sources per chunk: one pair per thread
   constexpr int kPairs = THREADS;
   constexpr int kFoldPairs = kPairs;
@@ -366,7 +369,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_interact_mixed(InteractParams
   __shared__ int s_ncp[2][THREADS / 32];  // per warp region: pairs on the hi/lo path
 
   const int tid = threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5, tbase = warp * 64;
+  const int lane = tid & 31, warp = tid >> 5, tbase = warp * 32;
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
@@ -415,10 +418,12 @@ __global__ void __launch_bounds__(THREADS, MINB) k_interact_mixed(InteractParams
       for (int c = 0; c < min(STAGES, n_chunks); ++c) issue(c);
     }
 
-    // This warp's targets: [tbase, tbase + 64) of the tile, nu of its two
-    // 32-target halves in use (warp-uniform), so a partly filled tile leaves
-    // its idle warps' issue slots to other blocks.
-    const int nu = w.t_count > tbase + 32 ? 2 : (w.t_count > tbase ? 1 : 0);
+    // This warp's targets: [tbase, tbase + 32) and [tbase + THREADS, tbase +
+    // THREADS + 32) of the tile, nu of the two in use (warp-uniform). A tile
+    // of up to THREADS targets gives every warp up to 32 of them, so a partly
+    // filled tile keeps all of the block's warps busy: the warps of a block sit
+    // on different SM sub-partitions, whose MUFU and FMA pipes are separate.
+    const int nu = w.t_count > tbase + THREADS ? 2 : (w.t_count > tbase ? 1 : 0);
 
     if (w.flags & kItemAudit) {
       // The audit's direct sum, in FP64 like the reference's
@@ -430,7 +435,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_interact_mixed(InteractParams
       double ax[TPT], ay[TPT], az[TPT], a64[TPT][NC];
 #pragma unroll
       for (int u = 0; u < TPT; ++u) {
-        const double4 t = p.T4a[w.t_begin + min(tbase + u * 32 + lane, w.t_count - 1)];
+        const double4 t = p.T4a[w.t_begin + min(tbase + u * THREADS + lane, w.t_count - 1)];
         ax[u] = t.x;
         ay[u] = t.y;
         az[u] = t.z;
@@ -470,7 +475,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_interact_mixed(InteractParams
       g += n_chunks;
 #pragma unroll
       for (int u = 0; u < TPT; ++u) {
-        const int i = tbase + u * 32 + lane;
+        const int i = tbase + u * THREADS + lane;
         if (i < w.t_count) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) atomicAdd(p.aout[c] + w.t_begin + i, a64[u][c] * p.scale[c]);
@@ -483,7 +488,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_interact_mixed(InteractParams
     double acc[TPT][NC], comp[TPT][NC];
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int i = min(tbase + u * 32 + lane, w.t_count - 1);
+      const int i = min(tbase + u * THREADS + lane, w.t_count - 1);
       const double4 t = p.T4[w.t_begin + i];
       float h, l;
       split_rel(t.x, w.cx, h, l);
@@ -651,7 +656,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_interact_mixed(InteractParams
 
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int i = tbase + u * 32 + lane;
+      const int i = tbase + u * THREADS + lane;
       if (i < w.t_count) {
         const int idx = p.T_out[w.t_begin + i];
 #pragma unroll
