@@ -44,6 +44,18 @@ SEED = 1
 FLOPS_PER_EVAL = {0: 13, 2: 24}
 
 
+def bench_config(kind):
+    """The workload both arms measure: the same object in the native and the
+    reference arm's line (the form each arm computes it with is reported
+    beside it, under "form")."""
+    what = "potential+gradient" if kind == 2 else "potential"
+    return {"workload": (f"3D Coulomb {what}, N={N_POINTS} uniform unit cube, charges U[-1,1], targets = sources, "
+                         f"n={DEGREE}, theta={THETA}, leaf {LEAF}, eps {EPS}"),
+            "tolerance_rel_l2": TOL,
+            "value_definition": "interactions of the plain fixed-degree solve of this workload (pairwise evaluations "
+                                "at n=8) divided by the solve time of the reported form"}
+
+
 def workload_name(kind, precision):
     what = "potential+gradient" if kind == 2 else "potential"
     prec = "plain FP64" if precision == 0 else "mixed FP32/FP64"
@@ -234,8 +246,10 @@ def run_reference(args, world, rank):
             "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64)",
             "impl": "reference",
-            "config": {"workload": workload_name(2, 0), "parallelism": "OpenMP host threads",
-                       "step": "a bounded sample of the solve (see cpu_baseline.sample)"},
+            "config": bench_config(2),
+            "form": {"name": "reference", "description": workload_name(2, 0) + " (the reference's own code)"},
+            "parallelism": "OpenMP host threads",
+            "step": "a bounded sample of the solve (see cpu_baseline.sample)",
             "cpu_baseline": {"value": value, "unit": "interactions/s", "cores": cores, "kind": "reference",
                              "sample": sample, "est_solve_s": statistics.median(ests),
                              "validated_ratio": val["validated_ratio"], "validation": val},
@@ -479,15 +493,14 @@ def run_native(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if headline == "plain" else "f32+f64",
         "data": "synthetic: seeded SplitMix64, uniform unit cube, charges U[-1,1]",
-        "config": {"workload": workload_name(kind, 0 if headline == "plain" else 1) +
-                   (", learned per-pair degrees 4..8 (adaptive pair tolerance; well-separated leaf pairs may be "
-                    "approximated) with 1% direct-sum audit" if headline == "learned" else ""),
-                   "form": headline, "tolerance_rel_l2": TOL,
-                   "value_definition": "interactions of the plain fixed-degree solve of this workload "
-                                       "(pairwise evaluations at n=8) divided by the solve time of the reported form",
-                   "l2": "flushed (256 MB write) before every step",
-                   "parallelism": "replicas" if world > 1 else "single GPU",
-                   "interactions_plain": plain_evals, "interactions_evaluated": H["evals"]},
+        "config": bench_config(kind),
+        "form": {"name": headline,
+                 "description": workload_name(kind, 0 if headline == "plain" else 1) +
+                 (", learned per-pair degrees 4..8 (adaptive pair tolerance; well-separated leaf pairs may be "
+                  "approximated) with 1% FP64 direct-sum audit" if headline == "learned" else ""),
+                 "interactions_plain": plain_evals, "interactions_evaluated": H["evals"]},
+        "l2": "flushed (256 MB write) before every step",
+        "parallelism": "replicas" if world > 1 else "single GPU",
         "forms": {n: {"ms_per_step": r["ms"], "interaction_kernel_ms": r["kernel_ms"], "evaluations": r["evals"],
                       "rel_l2_vs_direct_10k": acc[n], "setup_s": r["setup_s"],
                       "speedup_vs_plain_fp64": results["plain"]["ms"] / r["ms"] if "plain" in results else None}
