@@ -609,10 +609,11 @@ def run_configs(args, flush):
           500, plain FP64;
     cfg4: 3-D potential + gradient, N = 4,194,304 Plummer sphere (scale 0.1,
           r <= 2), charges U[0,1], leaf 2000, theta 0.7: learned + mixed at
-          tol 1e-6 against plain FP64 at n = 10;
+          tol 1e-6 against plain FP64 at n = 10, with mixed precision at fixed
+          n = 10 beside them;
     cfg5: the reference's 3-D vector kernel, eps 1e-3, N = 2,097,152 on the
-          unit sphere, strengths U[-1,1], leaf 2000, theta 0.8: learned + mixed
-          against plain FP64 at n = 10.
+          unit sphere, strengths U[-1,1], leaf 2000, theta 0.8: the same three
+          forms.
     Device times (CUDA events, L2 flushed before each solve); errors against
     the FP64 direct sum at 10,000 seeded targets. The learned form reports its
     first solve on a fresh plan (cold) and its time after 3 settling solves."""
@@ -633,6 +634,17 @@ def run_configs(args, flush):
         r = {"ms": statistics.median(ms), "evaluations": tc.evals(), "rel_l2_vs_direct_10k": rel_l2(o[:, idx], ds)}
         tc.close()
         return r, idx, ds
+
+    def mixed_leg(pts, q, kind, eps, theta, degree, leaf, idx, ds):
+        qd = torch.from_numpy(q).cuda()
+        tc = btk.Treecode(pts, degree=degree, cluster_size=leaf, theta=theta, eps=eps, kind=kind,
+                          precision=btk.PREC_MIXED, device_tree=True)
+        tc.solve(qd)
+        ms = [event_ms(lambda: tc.solve(qd), flush)[0] for _ in range(steps)]
+        o = tc.solve(qd).cpu().numpy()
+        r = {"ms": statistics.median(ms), "evaluations": tc.evals(), "rel_l2_vs_direct_10k": rel_l2(o[:, idx], ds)}
+        tc.close()
+        return r
 
     def learned_leg(pts, q, kind, eps, theta, degree, leaf, idx, ds):
         qd = torch.from_numpy(q).cuda()
@@ -667,10 +679,15 @@ def run_configs(args, flush):
              0.8)):
         pts, q = gen()
         plain, idx, ds = plain_leg(pts, q, kind, eps, theta, 10, 2000)
+        mixed = mixed_leg(pts, q, kind, eps, theta, 10, 2000, idx, ds)
+        mixed["speedup_vs_plain_fp64"] = plain["ms"] / mixed["ms"]
         learned = learned_leg(pts, q, kind, eps, theta, 10, 2000, idx, ds)
         learned["speedup_vs_plain_fp64"] = plain["ms"] / learned["ms"]
         learned["cold_speedup_vs_plain_fp64"] = plain["ms"] / learned["cold_first_solve_ms"]
-        out[key] = {"workload": what, "plain_fp64_n10": plain, "learned_mixed": learned, "tolerance_rel_l2": TOL}
+        # the learned solve's 1% FP64 direct-sum audit: N/100 targets x N sources
+        learned["evaluations_fp64_audit"] = (len(q) // 100) * len(q)
+        out[key] = {"workload": what, "plain_fp64_n10": plain, "mixed_n10": mixed, "learned_mixed": learned,
+                    "tolerance_rel_l2": TOL}
     return out
 
 
