@@ -247,7 +247,10 @@ def run_reference(args, world, rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64)",
             "impl": "reference",
             "config": bench_config(2),
-            "form": {"name": "reference", "description": workload_name(2, 0) + " (the reference's own code)"},
+            "form": {"name": "reference",
+                     "description": "the reference's own code, plain FP64 at n=8 on this workload: its potential pass "
+                                    "and its 3-D vector-kernel (velocity) pass, which stands in for the gradient (the "
+                                    "reference has no Coulomb-gradient kernel)"},
             "parallelism": "OpenMP host threads",
             "step": "a bounded sample of the solve (see cpu_baseline.sample)",
             "cpu_baseline": {"value": value, "unit": "interactions/s", "cores": cores, "kind": "reference",
