@@ -5,7 +5,8 @@
 For every size bucket 2^k <= N < 2^(k+1) (k = 12..17) it times batched solves
 of representative Gaussian-mixture problems (3-D Coulomb potential, degree 6,
 theta 0.6, mixed precision) at each candidate leaf size, then each work split
-at the best leaf size, and keeps the fastest pair (barytreek_b200.batch).
+at the best leaf size, then each tile size (targets per work item) at the best
+pair, and keeps the fastest (barytreek_b200.batch).
 """
 from __future__ import annotations
 
