@@ -310,7 +310,8 @@ __device__ __forceinline__ void eval_pair(const TargetPair& t, float2 nx, float2
 template <int DIM, int KIND, bool NEAR, int NU, int NC>
 __device__ __forceinline__ void pair_loop(const float4* fA, const float4* fB, const float4* fL, const float2* fLz,
                                           int j0, int j1, const TargetPair* T, float2 e2, float2 (*part)[NC]) {
-#pragma unroll 2
+  constexpr int kUnroll = NU == 1 ? 4 : 2;
+#pragma unroll kUnroll
   for (int j = j0; j < j1; ++j) {
     const float4 a = fA[j], b = fB[j];
     float4 l = make_float4(0.f, 0.f, 0.f, 0.f);
