@@ -311,12 +311,13 @@ template <int DIM, int KIND, bool NEAR, int NU, int NC>
 __device__ __forceinline__ void pair_loop(const float4* fA, const float4* fB, const float4* fL, const float2* fLz,
                                           int j0, int j1, const TargetPair* T, float2 e2, float2 (*part)[NC]) {
   // Source pairs in flight per warp (measured, 128-thread blocks): one target
-  // 4 (batch 269.3 -> 260.6 ms, learned 1M 40.9 -> 40.5 ms against 2); two
-  // targets 4 for potential + gradient (1M mixed 60.6 -> 59.9 ms), 3 for the
-  // potential (batch 260.6 -> 258.9 ms; 4 spills); the vector kernel keeps 2
-  // and 2 within its register budget at 5 blocks per SM.
+  // 4 (batch 269.3 -> 260.6 ms, learned 1M 40.9 -> 40.5 ms, 2M sphere vector
+  // kernel 68.4 -> 67.8 ms, against 2); two targets 4 for potential +
+  // gradient (1M mixed 60.6 -> 59.9 ms), 3 for the potential (batch 260.6 ->
+  // 258.9 ms; 4 spills), 2 for the vector kernel (its register budget at 5
+  // blocks per SM). The FP64 kernel's one-target loop measured slower at 4.
   constexpr int kUnroll =
-      KIND == BTK_KIND_VEL ? 2 : (NU == 1 ? 4 : (KIND == BTK_KIND_FIELD ? 4 : 3));
+      NU == 1 ? 4 : (KIND == BTK_KIND_FIELD ? 4 : (KIND == BTK_KIND_POT ? 3 : 2));
 #pragma unroll kUnroll
   for (int j = j0; j < j1; ++j) {
     const float4 a = fA[j], b = fB[j];
