@@ -312,12 +312,13 @@ __device__ __forceinline__ void pair_loop(const float4* fA, const float4* fB, co
                                           int j0, int j1, const TargetPair* T, float2 e2, float2 (*part)[NC]) {
   // Source pairs in flight per warp (measured, 128-thread blocks): one target
   // 4 (batch 269.3 -> 260.6 ms, learned 1M 40.9 -> 40.5 ms, 2M sphere vector
-  // kernel 68.4 -> 67.8 ms, against 2); two targets 4 for potential +
-  // gradient (1M mixed 60.6 -> 59.9 ms), 3 for the potential (batch 260.6 ->
-  // 258.9 ms; 4 spills), 2 for the vector kernel (its register budget at 5
-  // blocks per SM). The FP64 kernel's one-target loop measured slower at 4.
+  // kernel 68.4 -> 67.8 ms, against 2); two targets 6 for potential +
+  // gradient (1M mixed 60.6 -> 59.9 ms at 4, 59.6 ms at 6 or 8), 3 for the
+  // potential (batch 260.6 -> 258.9 ms; 4 spills), 2 for the vector kernel
+  // (its register budget at 5 blocks per SM). The FP64 kernel's one-target
+  // loop measured slower at 4.
   constexpr int kUnroll =
-      NU == 1 ? 4 : (KIND == BTK_KIND_FIELD ? 4 : (KIND == BTK_KIND_POT ? 3 : 2));
+      NU == 1 ? 4 : (KIND == BTK_KIND_FIELD ? 6 : (KIND == BTK_KIND_POT ? 3 : 2));
 #pragma unroll kUnroll
   for (int j = j0; j < j1; ++j) {
     const float4 a = fA[j], b = fB[j];
