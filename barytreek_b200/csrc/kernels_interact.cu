@@ -351,14 +351,13 @@ __device__ __forceinline__ void two_sum_add(double& sum, double& comp, double b)
   comp += e;
 }
 
-// Blocks per SM: potential + gradient 4 * 128 / THREADS (126 registers; at 5
-// blocks it spills); the vector kernel 5 * 128 / THREADS (96 registers, no
-// spills; 2M sphere learned solve 69.4 -> 68.3 ms against 4 blocks); the
-// potential alone 7 * 128 / THREADS with a
-// 2-stage ring (72 registers with a few bytes spilled outside the pair loop,
-// 30.8 KB of shared memory at 128 threads, so 7 blocks is also the
-// shared-memory limit; measured on the 256-problem batch: 5 blocks with 3
-// stages 299 ms, 6 blocks 280 ms, 7 blocks 270 ms).
+// Blocks per SM: potential + gradient 4 * 128 / THREADS (at most 128
+// registers; at 5 blocks it spills); the vector kernel 5 * 128 / THREADS (96
+// registers; 2M sphere learned solve 69.4 -> 68.3 ms against 4 blocks); the
+// potential alone 7 * 128 / THREADS with a 2-stage ring (72 registers with a
+// few bytes spilled, 30.8 KB of shared memory at 128 threads, so 7 blocks is
+// also the shared-memory limit; measured on the 256-problem batch: 5 blocks
+// with 3 stages 299 ms, 6 blocks 280 ms, 7 blocks 270 ms).
 template <int DIM, int KIND, int THREADS, int STAGES = KIND == BTK_KIND_POT ? 2 : kStages,
           int MINB = KIND == BTK_KIND_POT ? 7 * 128 / THREADS : (KIND == BTK_KIND_VEL ? 5 : 4) * 128 / THREADS>
 __global__ void __launch_bounds__(THREADS, MINB) k_interact_mixed(InteractParams p) {
